@@ -1,0 +1,449 @@
+// Direction-optimizing breadth-first search on the device (GIR::bfs, gir_query.cpp:108-294).
+//
+// Up to 64 queries run as one traversal: every vertex carries 64-bit lane masks (seen, current
+// frontier, next frontier), bit i standing for query i. A query's level of v is the iteration in
+// which its bit first reaches v, so every query gets exactly the levels a single-source BFS
+// gives it. One source per lane is GIR::bfs; several sources in a lane are the multi-source
+// query (all start at level 0).
+//
+// Each iteration runs in one of two directions, chosen per iteration by the schedule:
+//  - top-down: the frontier queue's out-edges are cut into equal chunks (edge-balanced, as the
+//    reference's 2048-edge chunks, gir_query.cpp:182-219); a lane bit newly reaching w is
+//    OR-ed into next[w] and w is queued once (the atomicOr that turns next[w] non-zero queues it);
+//  - bottom-up: every vertex that some lane has not reached ORs its in-neighbours' frontier
+//    masks and stops once every missing lane is found (gir_query.cpp:232-279), with vertices
+//    binned by in-degree: a thread, a warp or a CTA per vertex.
+#include "common.cuh"
+
+namespace gir {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kChunk = 32 * 16;  // edge positions per warp in the top-down expand
+
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+// counters: [0] queue length, [1] (vertex, lane) pairs reached this iteration,
+//           [2] out-edges of those pairs, [3] candidates queued by top-down
+enum { C_Q = 0, C_PAIRS = 1, C_MEDGES = 2, C_CAND = 3, C_N = 4 };
+
+__device__ __forceinline__ void write_levels(int32_t* level, int64_t V, int32_t v, uint64_t nb, int32_t L) {
+    while (nb) {
+        const int s = __ffsll((long long)nb) - 1;
+        nb &= nb - 1;
+        level[(int64_t)s * V + v] = L;
+    }
+}
+
+__device__ __forceinline__ void warp_add_u64(unsigned long long* p, unsigned long long x) {
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane_id() == 0 && x) atomicAdd(p, x);
+}
+
+// Sources: lane s of the group starts at every vertex of set s (set_beg is device memory).
+__global__ void k_init_sources(const int64_t* set_beg, int n_lanes, const int32_t* srcs, int64_t V, uint64_t* seen,
+                               uint64_t* front, int32_t* q, unsigned long long* cnt, int32_t* level) {
+    const int64_t lo = set_beg[0], hi = set_beg[n_lanes];
+    GRID_STRIDE(i, hi - lo) {
+        const int64_t e = lo + i;
+        int s = 0;  // lane of entry e
+        while (set_beg[s + 1] <= e) ++s;
+        const int32_t v = srcs[e];
+        if (v < 0 || v >= V) continue;
+        const uint64_t bit = 1ull << s;
+        atomicOr((unsigned long long*)&seen[v], bit);
+        const unsigned long long old = atomicOr((unsigned long long*)&front[v], bit);
+        level[(int64_t)s * V + v] = 0;
+        if (old == 0) q[atomicAdd(&cnt[C_Q], 1ull)] = v;
+    }
+}
+
+// Frontier out-degrees for the edge-balanced expand.
+__global__ void k_frontier_degrees(const int32_t* q, int64_t nq, const int32_t* deg, int64_t* pref) {
+    GRID_STRIDE(i, nq) pref[i] = deg[q[i]];
+    if (blockIdx.x == 0 && threadIdx.x == 0) pref[nq] = 0;
+}
+
+// Top-down: warp w takes edge positions [w*kChunk, (w+1)*kChunk) of the frontier's out-edges
+// (pref = exclusive scan of frontier degrees).
+__global__ void k_td_expand(const int32_t* q, int64_t nq, const int64_t* pref, int64_t total, CSRView fw,
+                            const uint64_t* front, const uint64_t* seen, uint64_t* next, int32_t* cand,
+                            unsigned long long* cnt) {
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c0 = warp * kChunk; c0 < total; c0 += nwarps * kChunk) {
+        const int64_t c1 = c0 + kChunk < total ? c0 + kChunk : total;
+        // frontier index owning this lane's first position (largest i with pref[i] <= p)
+        const int64_t key = c0 + lane < total ? c0 + lane : total - 1;
+        int64_t lo = 0, hi = nq - 1;
+        while (lo < hi) {
+            const int64_t m = (lo + hi + 1) >> 1;
+            if (pref[m] <= key) lo = m; else hi = m - 1;
+        }
+        int64_t i = lo;
+        for (int64_t base = c0; base < c1; base += 32) {  // warp-uniform
+            const int64_t p = base + lane;
+            bool fresh = false;
+            int32_t w = 0;
+            if (p < c1) {
+                while (pref[i + 1] <= p) ++i;
+                const int32_t u = q[i];
+                w = fw.adj[fw.beg[u] + (p - pref[i])];
+                const uint64_t bits = front[u] & ~seen[w];
+                if (bits) fresh = atomicOr((unsigned long long*)&next[w], (unsigned long long)bits) == 0ull;
+            }
+            warp_append(fresh, w, cand, &cnt[C_CAND]);
+        }
+    }
+}
+
+__global__ void k_clear_front(const int32_t* q, int64_t nq, uint64_t* front) {
+    GRID_STRIDE(i, nq) front[q[i]] = 0;
+}
+
+// Top-down commit: candidates become the new frontier with their newly reached lanes.
+__global__ void k_td_commit(const int32_t* cand, int64_t nc, uint64_t* seen, uint64_t* front, uint64_t* next,
+                            const int32_t* outdeg, int32_t* level, int64_t V, int32_t L, int32_t* q,
+                            unsigned long long* cnt) {
+    unsigned long long pairs = 0, medges = 0;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nc; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        bool on = false;
+        int32_t w = 0;
+        if (i < nc) {
+            w = cand[i];
+            const uint64_t s = seen[w];
+            const uint64_t nb = next[w] & ~s;
+            next[w] = 0;
+            if (nb) {
+                seen[w] = s | nb;
+                front[w] = nb;
+                write_levels(level, V, w, nb, L);
+                const unsigned c = __popcll(nb);
+                pairs += c;
+                medges += (unsigned long long)c * (unsigned long long)outdeg[w];
+                on = true;
+            }
+        }
+        warp_append(on, w, q, &cnt[C_Q]);
+    }
+    warp_add_u64(&cnt[C_PAIRS], pairs);
+    warp_add_u64(&cnt[C_MEDGES], medges);
+}
+
+// Bottom-up, thread per vertex (small in-degree bin).
+__global__ void k_bu_thread(const int32_t* ids, int64_t n, CSRView bw, const uint64_t* front, uint64_t* seen,
+                            uint64_t* next, uint64_t all, const int32_t* outdeg, int32_t* level, int64_t V,
+                            int32_t L, int32_t* q, unsigned long long* cnt) {
+    unsigned long long pairs = 0, medges = 0;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        bool on = false;
+        int32_t v = 0;
+        if (i < n) {
+            v = ids[i];
+            const uint64_t s = seen[v];
+            const uint64_t want = all & ~s;
+            uint64_t nb = 0;
+            if (want) {
+                uint64_t acc = 0;
+                const int64_t b = bw.beg[v], e = b + bw.deg[v];
+                for (int64_t k = b; k < e; ++k) {
+                    acc |= front[bw.adj[k]];
+                    if ((acc & want) == want) break;
+                }
+                nb = acc & want;
+            }
+            next[v] = nb;
+            if (nb) {
+                seen[v] = s | nb;
+                write_levels(level, V, v, nb, L);
+                const unsigned c = __popcll(nb);
+                pairs += c;
+                medges += (unsigned long long)c * (unsigned long long)outdeg[v];
+                on = true;
+            }
+        }
+        warp_append(on, v, q, &cnt[C_Q]);
+    }
+    warp_add_u64(&cnt[C_PAIRS], pairs);
+    warp_add_u64(&cnt[C_MEDGES], medges);
+}
+
+__device__ __forceinline__ uint64_t warp_or_u64(uint64_t x) {
+    const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)(x & 0xffffffffu));
+    const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(x >> 32));
+    return ((uint64_t)hi << 32) | lo;
+}
+
+// Bottom-up, warp per vertex (medium bin): lanes read 32 consecutive in-neighbours per round.
+__global__ void k_bu_warp(const int32_t* ids, int64_t n, CSRView bw, const uint64_t* front, uint64_t* seen,
+                          uint64_t* next, uint64_t all, const int32_t* outdeg, int32_t* level, int64_t V, int32_t L,
+                          int32_t* q, unsigned long long* cnt) {
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long pairs = 0, medges = 0;
+    for (int64_t i = warp; i < n; i += nwarps) {
+        const int32_t v = ids[i];
+        const uint64_t s = seen[v];
+        const uint64_t want = all & ~s;
+        uint64_t nb = 0;
+        if (want) {
+            uint64_t acc = 0;
+            const int64_t b = bw.beg[v], e = b + bw.deg[v];
+            for (int64_t k0 = b; k0 < e; k0 += 32) {
+                const int64_t k = k0 + lane;
+                uint64_t a = k < e ? front[bw.adj[k]] : 0ull;
+                acc |= warp_or_u64(a);
+                if ((acc & want) == want) break;
+            }
+            nb = acc & want;
+        }
+        if (lane == 0) {
+            next[v] = nb;
+            if (nb) {
+                seen[v] = s | nb;
+                const unsigned c = __popcll(nb);
+                pairs += c;
+                medges += (unsigned long long)c * (unsigned long long)outdeg[v];
+                q[atomicAdd(&cnt[C_Q], 1ull)] = v;
+            }
+        }
+        // lanes split the level writes of this vertex
+        uint64_t rest = nb;
+        for (int j = 0; rest; ++j) {
+            const int sbit = __ffsll((long long)rest) - 1;
+            rest &= rest - 1;
+            if ((j & 31) == lane) level[(int64_t)sbit * V + v] = L;
+        }
+    }
+    if (lane == 0) {
+        if (pairs) atomicAdd(&cnt[C_PAIRS], pairs);
+        if (medges) atomicAdd(&cnt[C_MEDGES], medges);
+    }
+}
+
+// Bottom-up, CTA per vertex (large bin).
+__global__ void k_bu_cta(const int32_t* ids, int64_t n, CSRView bw, const uint64_t* front, uint64_t* seen,
+                         uint64_t* next, uint64_t all, const int32_t* outdeg, int32_t* level, int64_t V, int32_t L,
+                         int32_t* q, unsigned long long* cnt) {
+    __shared__ unsigned long long s_acc;
+    for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int32_t v = ids[i];
+        const uint64_t s = seen[v];
+        const uint64_t want = all & ~s;
+        if (threadIdx.x == 0) s_acc = 0;
+        __syncthreads();
+        if (want) {
+            const int64_t b = bw.beg[v], e = b + bw.deg[v];
+            for (int64_t k0 = b; k0 < e; k0 += blockDim.x) {
+                const int64_t k = k0 + threadIdx.x;
+                uint64_t a = k < e ? front[bw.adj[k]] : 0ull;
+                a = warp_or_u64(a);
+                if (lane_id() == 0 && (a & want)) atomicOr(&s_acc, (unsigned long long)(a & want));
+                __syncthreads();
+                const bool done = (s_acc & want) == want;
+                __syncthreads();
+                if (done) break;
+            }
+        }
+        const uint64_t nb = s_acc & want;
+        if (threadIdx.x == 0) {
+            next[v] = nb;
+            if (nb) {
+                seen[v] = s | nb;
+                const unsigned c = __popcll(nb);
+                atomicAdd(&cnt[C_PAIRS], (unsigned long long)c);
+                atomicAdd(&cnt[C_MEDGES], (unsigned long long)c * (unsigned long long)outdeg[v]);
+                q[atomicAdd(&cnt[C_Q], 1ull)] = v;
+            }
+        }
+        if (threadIdx.x < 64 && ((nb >> threadIdx.x) & 1ull)) level[(int64_t)threadIdx.x * V + v] = L;
+        __syncthreads();
+    }
+}
+
+// Out-edges of the sources' lanes, for the traversed-edge count.
+__global__ void k_source_edges(const int32_t* q, int64_t nq, const uint64_t* front, const int32_t* outdeg,
+                               unsigned long long* cnt) {
+    unsigned long long pairs = 0, medges = 0;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nq; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        if (i < nq) {
+            const int32_t v = q[i];
+            const unsigned c = __popcll(front[v]);
+            pairs += c;
+            medges += (unsigned long long)c * (unsigned long long)outdeg[v];
+        }
+    }
+    warp_add_u64(&cnt[C_PAIRS], pairs);
+    warp_add_u64(&cnt[C_MEDGES], medges);
+}
+
+}  // namespace
+
+int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t n_sets, int32_t* level_d) {
+    const int64_t V = g->V;
+    QueryStats& st = g->qstats;
+    st = QueryStats{};
+    if (n_sets <= 0) return GIR_OK;
+    GIR_CUDA(g, cudaMemsetAsync(level_d, 0xff, sizeof(int32_t) * V * n_sets, g->stream));
+    if (V == 0) return GIR_OK;
+    if (!g->bins_valid) GIR_TRY(store_build_bins(g));
+
+    uint64_t *seen = nullptr, *front = nullptr, *next = nullptr;
+    int32_t *qa = nullptr, *qb = nullptr;
+    int64_t *pref = nullptr, *sbeg = nullptr;
+    unsigned long long* cnt = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[0], V, &seen));
+    GIR_TRY(ensure_n(g, g->scratch[1], V, &front));
+    GIR_TRY(ensure_n(g, g->scratch[2], V, &next));
+    GIR_TRY(ensure_n(g, g->scratch[3], V + 1, &qa));
+    GIR_TRY(ensure_n(g, g->scratch[4], V + 1, &qb));
+    GIR_TRY(ensure_n(g, g->scratch[5], V + 2, &pref));
+    GIR_TRY(ensure_n(g, g->scratch[6], 65, &sbeg));
+    GIR_TRY(ensure_n(g, g->scratch[7], C_N, &cnt));
+    unsigned long long* hc = nullptr;
+    {
+        void* h = nullptr;
+        GIR_TRY(pinned(g, 256, &h));
+        hc = static_cast<unsigned long long*>(h);
+    }
+    const double alpha = g->params[GIR_PARAM_ALPHA], beta = g->params[GIR_PARAM_BETA];
+    const int64_t E = g->fw.E;
+    const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
+    GIR_CUDA(g, cudaEventRecord(g->ev0, g->stream));
+
+    for (int64_t g0 = 0; g0 < n_sets; g0 += 64) {
+        const int nl = (int)((n_sets - g0) < 64 ? (n_sets - g0) : 64);
+        const uint64_t all = nl == 64 ? ~0ull : ((1ull << nl) - 1);
+        int32_t* level = level_d + g0 * V;
+        GIR_CUDA(g, cudaMemsetAsync(seen, 0, sizeof(uint64_t) * V, g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(front, 0, sizeof(uint64_t) * V, g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(next, 0, sizeof(uint64_t) * V, g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+        GIR_CUDA(g, cudaMemcpyAsync(sbeg, set_beg_h + g0, sizeof(int64_t) * (nl + 1), cudaMemcpyHostToDevice, g->stream));
+        const int64_t n_entries = set_beg_h[g0 + nl] - set_beg_h[g0];
+        if (n_entries > 0) {
+            k_init_sources<<<grid_for(g, n_entries, kBlock), kBlock, 0, g->stream>>>(sbeg, nl, srcs_d, V, seen, front, qa,
+                                                                                     cnt, level);
+            GIR_LAUNCH(g, "k_init_sources");
+            st.launches++;
+        }
+        GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+        int64_t nq = (int64_t)hc[0];
+        if (nq > 0) {
+            k_source_edges<<<grid_for(g, nq, kBlock), kBlock, 0, g->stream>>>(qa, nq, front, g->fw.deg, cnt);
+            GIR_LAUNCH(g, "k_source_edges");
+            st.launches++;
+            GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+        }
+        double mf = (double)hc[C_MEDGES] / nl;       // out-edges of the frontier (per lane)
+        double nf = (double)hc[C_PAIRS] / nl;        // frontier vertices (per lane)
+        double mu = (double)E - mf;                  // out-edges not yet explored (per lane)
+        st.edges += (int64_t)hc[C_MEDGES];
+        st.reached += (int64_t)hc[C_PAIRS];
+        bool bottom_up = false, next_dirty = false;
+        int32_t L = 0;
+        while (nq > 0) {
+            // direction (the reference's switch, gir_query.cpp:159-169, or the schedule network)
+            if (V >= 4096) {
+                if (g->schedule == GIR_SCHEDULE_LEARNED && g->sched_loaded) {
+                    float feat[GIR_SCHED_IN] = {(float)(nf / V), (float)(mf / (E + 1.0)), (float)(mu / (E + 1.0)),
+                                                (float)((double)L / 64.0), bottom_up ? 1.f : 0.f,
+                                                (float)((double)E / V / 64.0), (float)(nl / 64.0), 1.f};
+                    int bu = bottom_up;
+                    GIR_TRY(sched_choose_direction(g, feat, bottom_up, &bu));
+                    bottom_up = bu != 0;
+                } else {
+                    if (!bottom_up && mf * alpha > mu) bottom_up = true;
+                    else if (bottom_up && nf * beta < (double)V) bottom_up = false;
+                }
+            }
+            GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+            if (!bottom_up) {
+                if (next_dirty) {
+                    GIR_CUDA(g, cudaMemsetAsync(next, 0, sizeof(uint64_t) * V, g->stream));
+                    next_dirty = false;
+                }
+                k_frontier_degrees<<<grid_for(g, nq, kBlock), kBlock, 0, g->stream>>>(qa, nq, g->fw.deg, pref);
+                GIR_LAUNCH(g, "k_frontier_degrees");
+                GIR_TRY(exclusive_scan_i64(g, pref, pref, nq + 1));
+                int64_t total = 0;
+                GIR_CUDA(g, cudaMemcpyAsync(&hc[8], pref + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
+                GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+                total = (int64_t)hc[8];
+                if (total > 0) {
+                    const int64_t chunks = (total + kChunk - 1) / kChunk;
+                    const int64_t warps_per_block = kBlock / 32;
+                    int64_t blocks = (chunks + warps_per_block - 1) / warps_per_block;
+                    if (blocks > grid) blocks = grid;
+                    k_td_expand<<<(int)blocks, kBlock, 0, g->stream>>>(qa, nq, pref, total, view(g->fw), front, seen,
+                                                                       next, qb, cnt);
+                    GIR_LAUNCH(g, "k_td_expand");
+                }
+                k_clear_front<<<grid_for(g, nq, kBlock), kBlock, 0, g->stream>>>(qa, nq, front);
+                GIR_LAUNCH(g, "k_clear_front");
+                GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+                GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+                const int64_t nc = (int64_t)hc[C_CAND];
+                if (nc > 0) {
+                    k_td_commit<<<grid_for(g, nc, kBlock), kBlock, 0, g->stream>>>(qb, nc, seen, front, next, g->fw.deg,
+                                                                                   level, V, L + 1, qa, cnt);
+                    GIR_LAUNCH(g, "k_td_commit");
+                }
+                st.launches += 4;
+            } else {
+                const int32_t* bins = static_cast<const int32_t*>(g->bins.p);
+                if (g->bin_n[0] > 0) {
+                    k_bu_thread<<<grid_for(g, g->bin_n[0], kBlock), kBlock, 0, g->stream>>>(
+                        bins, g->bin_n[0], view(g->bw), front, seen, next, all, g->fw.deg, level, V, L + 1, qa, cnt);
+                    GIR_LAUNCH(g, "k_bu_thread");
+                    st.launches++;
+                }
+                if (g->bin_n[1] > 0) {
+                    k_bu_warp<<<grid_for(g, g->bin_n[1] * 32, kBlock), kBlock, 0, g->stream>>>(
+                        bins + g->bin_n[0], g->bin_n[1], view(g->bw), front, seen, next, all, g->fw.deg, level, V, L + 1,
+                        qa, cnt);
+                    GIR_LAUNCH(g, "k_bu_warp");
+                    st.launches++;
+                }
+                if (g->bin_n[2] > 0) {
+                    const int64_t b = g->bin_n[2] < grid ? g->bin_n[2] : grid;
+                    k_bu_cta<<<(int)b, kBlock, 0, g->stream>>>(bins + g->bin_n[0] + g->bin_n[1], g->bin_n[2],
+                                                               view(g->bw), front, seen, next, all, g->fw.deg, level, V,
+                                                               L + 1, qa, cnt);
+                    GIR_LAUNCH(g, "k_bu_cta");
+                    st.launches++;
+                }
+                std::swap(front, next);
+                next_dirty = true;
+                st.bottom_up++;
+            }
+            GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+            nq = (int64_t)hc[C_Q];
+            mf = (double)hc[C_MEDGES] / nl;
+            nf = (double)hc[C_PAIRS] / nl;
+            mu -= mf;
+            st.edges += (int64_t)hc[C_MEDGES];
+            st.reached += (int64_t)hc[C_PAIRS];
+            ++L;
+            st.iterations++;
+        }
+    }
+    GIR_CUDA(g, cudaEventRecord(g->ev1, g->stream));
+    GIR_CUDA(g, cudaEventSynchronize(g->ev1));
+    float ms = 0;
+    GIR_CUDA(g, cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    st.kernel_ms = ms;
+    return GIR_OK;
+}
+
+}  // namespace gir

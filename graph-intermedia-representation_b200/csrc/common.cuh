@@ -1,0 +1,273 @@
+// Internal declarations shared by the GIR-B200 CUDA sources: the handle, the device graph
+// store, scratch buffers, error plumbing and small device helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "gir_dev.h"
+
+namespace gir {
+
+// ---------------------------------------------------------------------------------------------
+// Error plumbing: every internal function returns a gir status; the first failure records its
+// text in the handle.
+// ---------------------------------------------------------------------------------------------
+struct Status {
+    int code = GIR_OK;
+    std::string msg;
+};
+
+#define GIR_TRY(expr)                    \
+    do {                                 \
+        int _rc = (expr);                \
+        if (_rc != GIR_OK) return _rc;   \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Slack CSR resident in HBM. Row v holds deg[v] sorted neighbour ids at adj[beg[v] ..
+// beg[v] + deg[v]); the rest of [beg[v], beg[v+1]) is free room for inserts. Every row starts
+// on a 16-byte boundary (beg[v] % 4 == 0) so rows can be read with 128-bit loads.
+// ---------------------------------------------------------------------------------------------
+struct DevCSR {
+    int64_t* beg = nullptr;  // V + 1 capacity offsets
+    int32_t* deg = nullptr;  // V current row lengths
+    int32_t* adj = nullptr;  // beg[V] entries
+    uint32_t* w = nullptr;   // optional weights aligned with adj
+    int64_t cap = 0;         // beg[V]
+    int64_t E = 0;           // sum of deg
+};
+
+// Device view passed to kernels by value.
+struct CSRView {
+    const int64_t* beg;
+    const int32_t* deg;
+    const int32_t* adj;
+    const uint32_t* w;
+};
+inline CSRView view(const DevCSR& c) { return CSRView{c.beg, c.deg, c.adj, c.w}; }
+
+struct QueryStats {
+    int64_t edges = 0, reached = 0, iterations = 0, bottom_up = 0, launches = 0;
+    double kernel_ms = 0, total_ms = 0;
+};
+
+}  // namespace gir
+
+// The handle. (Global namespace: the C ABI forward-declares `struct gir_dev`.)
+struct gir_dev {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+    int64_t V = 0;
+
+    gir::DevCSR fw, bw, sym;
+    bool has_weights = false;
+    uint64_t wrule_seed = 0;
+    uint32_t wrule_lo = 0, wrule_hi = 0;  // lo > hi: use the hash weight of GIR::edgeWeight
+
+    // Layers
+    bool wcc_built = false, scc_built = false, bct_built = false;
+    gir::DevBuf wcc, scc, scc_rank;  // int32[V]
+    int64_t n_wcc = -1, n_scc = -1;
+    gir::DevBuf dag;                 // uint64 keys (scc_u << 32 | scc_v), sorted, distinct
+    int64_t n_dag = -1;
+    gir::DevBuf blk_label, blk_head, bcnt;  // int32[V], int32[n_blocks], int32[V]
+    int64_t n_blocks = -1;
+
+    // Weight-sorted copies of the forward CSR for SSSP ([0] hash weights, [1] stored weights).
+    gir::DevCSR ws[2];
+    bool ws_valid[2] = {false, false};
+
+    // Degree bins of the backward CSR (bottom-up traversal): vertex ids by in-degree class.
+    gir::DevBuf bins;                // int32[V]: small | medium | large, each ascending
+    int64_t bin_n[3] = {0, 0, 0};
+    bool bins_valid = false;
+
+    // Scratch, grown on demand and kept across calls.
+    gir::DevBuf scratch[16];
+    gir::DevBuf cub_tmp;
+    gir::DevBuf stage_in, stage_out;  // device staging for host pointers
+    gir::DevBuf work[8];              // buffers of the create / batch pipelines (not used by store ops)
+    void* pinned = nullptr;           // small pinned host buffer for counters
+    size_t pinned_bytes = 0;
+
+    // Batch statistics
+    int64_t b_ins = 0, b_del = 0, b_noop = 0, b_invalid = 0;
+
+    // Schedule
+    int schedule = GIR_SCHEDULE_FIXED;
+    double params[GIR_PARAM_COUNT] = {15.0, 18.0, 16.0, 256.0, 32.0, 4096.0, 4.0};
+    gir::DevBuf sched_w;              // MLP parameters (fp32)
+    gir::DevBuf sched_io;             // one decision's features and logits
+    bool sched_loaded = false;
+    std::vector<float> sched_host;    // host copy of the MLP parameters
+
+    gir::QueryStats qstats;
+    std::string err;
+};
+
+namespace gir {
+
+// Records an error on the handle and returns `code`.
+int fail(gir_dev* g, int code, const std::string& msg);
+// Checks a CUDA result; on failure records it and returns GIR_ERR_CUDA (or GIR_ERR_OOM).
+int cuda_check(gir_dev* g, cudaError_t e, const char* what);
+#define GIR_CUDA(g, call) GIR_TRY(::gir::cuda_check((g), (call), #call))
+#define GIR_LAUNCH(g, what) GIR_TRY(::gir::cuda_check((g), cudaGetLastError(), what))
+
+// Grows a device buffer to at least `bytes` (contents not kept).
+int ensure(gir_dev* g, DevBuf& b, size_t bytes);
+template <class T>
+int ensure_n(gir_dev* g, DevBuf& b, size_t n, T** out) {
+    GIR_TRY(ensure(g, b, n * sizeof(T) + 16));
+    *out = static_cast<T*>(b.p);
+    return GIR_OK;
+}
+void release(DevBuf& b);
+
+// Pinned host scratch of at least `bytes`.
+int pinned(gir_dev* g, size_t bytes, void** out);
+
+bool is_device_ptr(const void* p);
+
+// Copies `bytes` from a host or device pointer into device memory owned by the handle
+// (`stage`), or returns `p` itself when it is already device memory.
+int stage_input(gir_dev* g, DevBuf& stage, const void* p, size_t bytes, const void** dev);
+
+// Grid size for a persistent/grid-stride kernel.
+inline int grid_for(gir_dev* g, int64_t work, int block) {
+    const int64_t blocks = (work + block - 1) / block;
+    const int64_t cap = (int64_t)g->num_sms * (int64_t)g->params[GIR_PARAM_CTAS_PER_SM] * 4;
+    return (int)(blocks < 1 ? 1 : (blocks < cap ? blocks : cap));
+}
+
+// ---- store (store.cu) ----
+int store_build_csr_from_keys(gir_dev* g, DevCSR& c, const uint64_t* keys, int64_t n, const uint32_t* w);
+int store_free(DevCSR& c);
+int store_build_sym(gir_dev* g);
+int store_compact_csr(gir_dev* g, const DevCSR& c, int64_t* beg_out, int32_t* adj_out, int64_t cap);
+int store_has_edges(gir_dev* g, const DevCSR& c, const int32_t* u, const int32_t* v, int64_t n, uint8_t* out);
+int store_apply_ops(gir_dev* g, DevCSR& c, const uint64_t* ins, int64_t n_ins, const uint64_t* del, int64_t n_del,
+                    bool weights);
+int store_build_bins(gir_dev* g);
+
+// ---- CUB wrappers (prims.cu) ----
+int sort_keys_u64(gir_dev* g, uint64_t* keys, uint64_t* tmp, int64_t n, int end_bit);
+int sort_pairs_u64(gir_dev* g, uint64_t* keys, uint64_t* ktmp, uint32_t* vals, uint32_t* vtmp, int64_t n, int end_bit);
+int sort_pairs_u64_i64(gir_dev* g, uint64_t* keys, uint64_t* ktmp, int64_t* vals, int64_t* vtmp, int64_t n, int end_bit);
+int exclusive_scan_i64(gir_dev* g, const int64_t* in, int64_t* out, int64_t n);
+int sum_i64(gir_dev* g, const int64_t* in, int64_t n, int64_t* host_out);
+// Compacts the entries of `in` whose flag is non-zero into `out`; *host_n = count.
+int select_flagged_u64(gir_dev* g, const uint64_t* in, const uint8_t* flags, uint64_t* out, int64_t n, int64_t* host_n);
+int select_flagged_i32(gir_dev* g, const int32_t* in, const uint8_t* flags, int32_t* out, int64_t n, int64_t* host_n);
+// Indices i in [0, n) with flags[i] != 0, ascending.
+int select_flagged_iota(gir_dev* g, const uint8_t* flags, int32_t* out, int64_t n, int64_t* host_n);
+
+// ---- layers ----
+// Components of the undirected view of a forward CSR; label = smallest vertex id (wcc.cu).
+int wcc_labels(gir_dev* g, const DevCSR& c, int32_t* label, int64_t* n_comp);
+int wcc_build(gir_dev* g);
+int scc_build(gir_dev* g);
+int bct_build(gir_dev* g);
+
+// ---- queries ----
+int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t n_sets, int32_t* level_d);
+int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t n_sets, uint64_t delta,
+             int weight_mode, uint64_t* dist_d);
+
+// ---- schedule network (sched.cu) ----
+int sched_choose_delta(gir_dev* g, const float* features, uint64_t* delta);
+int sched_choose_direction(gir_dev* g, const float* features, int current, int* bottom_up);
+
+// ---------------------------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------------------------
+#ifdef __CUDACC__
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// GIR::edgeWeight (gir_query.cpp:50-54): MurmurHash3's fmix64 of (u << 32 | v) into [1,100].
+__device__ __forceinline__ uint32_t hash_weight(int32_t u, int32_t v) {
+    uint64_t x = ((uint64_t)(uint32_t)u << 32) | (uint32_t)v;
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdULL; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
+    return 1u + (uint32_t)(x % 100ull);
+}
+
+// Lower bound of `x` in the sorted range a[lo, hi).
+template <class T>
+__device__ __forceinline__ int64_t lower_bound_dev(const T* a, int64_t lo, int64_t hi, T x) {
+    while (lo < hi) {
+        const int64_t m = (lo + hi) >> 1;
+        if (a[m] < x) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
+// Calls f(u, w, edge_index) for every entry of the rows of vertices [v0, v1) of `c`. Warp-
+// cooperative: a warp takes 32 consecutive vertices, scans their row lengths and walks the
+// concatenated rows 32 entries at a time (consecutive lanes read consecutive entries of a row),
+// so a row of any length costs its warp ceil(len/32) rounds. Must be called by all threads of
+// the grid (every lane of a warp takes part in every round). `scan` is per-warp shared scratch
+// of 33 int64 and 32 int32.
+template <class F>
+__device__ __forceinline__ void warp_sweep_rows(const int64_t* beg, const int32_t* deg, const int32_t* adj,
+                                                int64_t v0, int64_t v1, int64_t* s_excl, int32_t* s_u, F&& f) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = v0 + warp * 32; base < v1; base += nwarps * 32) {
+        const int64_t v = base + lane;
+        const int64_t cnt = v < v1 ? deg[v] : 0;
+        int64_t incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        s_excl[lane] = incl - cnt;
+        if (lane == 31) s_excl[32] = incl;
+        s_u[lane] = (int32_t)v;
+        __syncwarp();
+        const int64_t total = s_excl[32];
+        for (int64_t p0 = 0; p0 < total; p0 += 32) {
+            const int64_t p = p0 + lane;
+            if (p < total) {
+                int lo = 0, hi = 31;
+                while (lo < hi) {
+                    const int m = (lo + hi + 1) >> 1;
+                    if (s_excl[m] <= p) lo = m; else hi = m - 1;
+                }
+                const int32_t u = s_u[lo];
+                const int64_t e = beg[u] + (p - s_excl[lo]);
+                f(u, adj[e], e);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Warp-aggregated append: every lane with `pred` gets a distinct slot in `q` (counter `cnt`).
+__device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t* q, unsigned long long* cnt) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane_id() == leader) base = atomicAdd(cnt, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) q[base + __popc(m & ((1u << lane_id()) - 1))] = value;
+}
+#endif
+
+}  // namespace gir

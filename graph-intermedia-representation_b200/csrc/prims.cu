@@ -1,0 +1,170 @@
+// Handle utilities (errors, buffers, staging) and the sort / scan / compaction primitives of
+// the build and update pipelines. The primitives are CUB's device-wide algorithms (header-only
+// templates from the CUDA toolkit, instantiated here for sm_100a); the traversal kernels of
+// the hot path are this library's own.
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+
+namespace gir {
+
+int fail(gir_dev* g, int code, const std::string& msg) {
+    if (g) g->err = msg;
+    return code;
+}
+
+int cuda_check(gir_dev* g, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return GIR_OK;
+    const int code = (e == cudaErrorMemoryAllocation) ? GIR_ERR_OOM : GIR_ERR_CUDA;
+    cudaGetLastError();  // clear a non-sticky error
+    return fail(g, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int ensure(gir_dev* g, DevBuf& b, size_t bytes) {
+    if (b.bytes >= bytes && b.p) return GIR_OK;
+    if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+    size_t want = bytes < 256 ? 256 : bytes;
+    want = (want + 255) & ~(size_t)255;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        cudaGetLastError();
+        return fail(g, GIR_ERR_OOM, "device allocation of " + std::to_string(want) + " bytes failed: " +
+                                        cudaGetErrorString(e));
+    }
+    b.bytes = want;
+    return GIR_OK;
+}
+
+void release(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+int pinned(gir_dev* g, size_t bytes, void** out) {
+    if (g->pinned_bytes < bytes) {
+        if (g->pinned) cudaFreeHost(g->pinned);
+        g->pinned = nullptr;
+        g->pinned_bytes = 0;
+        GIR_CUDA(g, cudaMallocHost(&g->pinned, bytes));
+        g->pinned_bytes = bytes;
+    }
+    *out = g->pinned;
+    return GIR_OK;
+}
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int stage_input(gir_dev* g, DevBuf& stage, const void* p, size_t bytes, const void** dev) {
+    if (bytes == 0) { *dev = p; return GIR_OK; }
+    if (is_device_ptr(p)) { *dev = p; return GIR_OK; }
+    GIR_TRY(ensure(g, stage, bytes));
+    GIR_CUDA(g, cudaMemcpyAsync(stage.p, p, bytes, cudaMemcpyHostToDevice, g->stream));
+    *dev = stage.p;
+    return GIR_OK;
+}
+
+int sort_keys_u64(gir_dev* g, uint64_t* keys, uint64_t* tmp, int64_t n, int end_bit) {
+    if (n <= 1) return GIR_OK;
+    cub::DoubleBuffer<uint64_t> kb(keys, tmp);
+    size_t bytes = 0;
+    GIR_CUDA(g, cub::DeviceRadixSort::SortKeys(nullptr, bytes, kb, n, 0, end_bit, g->stream));
+    GIR_TRY(ensure(g, g->cub_tmp, bytes));
+    GIR_CUDA(g, cub::DeviceRadixSort::SortKeys(g->cub_tmp.p, bytes, kb, n, 0, end_bit, g->stream));
+    if (kb.Current() != keys)
+        GIR_CUDA(g, cudaMemcpyAsync(keys, kb.Current(), sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, g->stream));
+    return GIR_OK;
+}
+
+int sort_pairs_u64(gir_dev* g, uint64_t* keys, uint64_t* ktmp, uint32_t* vals, uint32_t* vtmp, int64_t n, int end_bit) {
+    if (n <= 1) return GIR_OK;
+    cub::DoubleBuffer<uint64_t> kb(keys, ktmp);
+    cub::DoubleBuffer<uint32_t> vb(vals, vtmp);
+    size_t bytes = 0;
+    GIR_CUDA(g, cub::DeviceRadixSort::SortPairs(nullptr, bytes, kb, vb, n, 0, end_bit, g->stream));
+    GIR_TRY(ensure(g, g->cub_tmp, bytes));
+    GIR_CUDA(g, cub::DeviceRadixSort::SortPairs(g->cub_tmp.p, bytes, kb, vb, n, 0, end_bit, g->stream));
+    if (kb.Current() != keys)
+        GIR_CUDA(g, cudaMemcpyAsync(keys, kb.Current(), sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, g->stream));
+    if (vb.Current() != vals)
+        GIR_CUDA(g, cudaMemcpyAsync(vals, vb.Current(), sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, g->stream));
+    return GIR_OK;
+}
+
+int sort_pairs_u64_i64(gir_dev* g, uint64_t* keys, uint64_t* ktmp, int64_t* vals, int64_t* vtmp, int64_t n, int end_bit) {
+    if (n <= 1) return GIR_OK;
+    cub::DoubleBuffer<uint64_t> kb(keys, ktmp);
+    cub::DoubleBuffer<int64_t> vb(vals, vtmp);
+    size_t bytes = 0;
+    GIR_CUDA(g, cub::DeviceRadixSort::SortPairs(nullptr, bytes, kb, vb, n, 0, end_bit, g->stream));
+    GIR_TRY(ensure(g, g->cub_tmp, bytes));
+    GIR_CUDA(g, cub::DeviceRadixSort::SortPairs(g->cub_tmp.p, bytes, kb, vb, n, 0, end_bit, g->stream));
+    if (kb.Current() != keys)
+        GIR_CUDA(g, cudaMemcpyAsync(keys, kb.Current(), sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, g->stream));
+    if (vb.Current() != vals)
+        GIR_CUDA(g, cudaMemcpyAsync(vals, vb.Current(), sizeof(int64_t) * n, cudaMemcpyDeviceToDevice, g->stream));
+    return GIR_OK;
+}
+
+int exclusive_scan_i64(gir_dev* g, const int64_t* in, int64_t* out, int64_t n) {
+    if (n <= 0) return GIR_OK;
+    size_t bytes = 0;
+    GIR_CUDA(g, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, g->stream));
+    GIR_TRY(ensure(g, g->cub_tmp, bytes));
+    GIR_CUDA(g, cub::DeviceScan::ExclusiveSum(g->cub_tmp.p, bytes, in, out, n, g->stream));
+    return GIR_OK;
+}
+
+int sum_i64(gir_dev* g, const int64_t* in, int64_t n, int64_t* host_out) {
+    int64_t* d_out = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[15], 1, &d_out));
+    if (n <= 0) { *host_out = 0; return GIR_OK; }
+    size_t bytes = 0;
+    GIR_CUDA(g, cub::DeviceReduce::Sum(nullptr, bytes, in, d_out, n, g->stream));
+    GIR_TRY(ensure(g, g->cub_tmp, bytes));
+    GIR_CUDA(g, cub::DeviceReduce::Sum(g->cub_tmp.p, bytes, in, d_out, n, g->stream));
+    void* h = nullptr;
+    GIR_TRY(pinned(g, 64, &h));
+    GIR_CUDA(g, cudaMemcpyAsync(h, d_out, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    *host_out = *static_cast<int64_t*>(h);
+    return GIR_OK;
+}
+
+template <class It, class T>
+static int select_flagged(gir_dev* g, It in, const uint8_t* flags, T* out, int64_t n, int64_t* host_n) {
+    int64_t* d_n = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[15], 1, &d_n));
+    if (n <= 0) { *host_n = 0; return GIR_OK; }
+    size_t bytes = 0;
+    GIR_CUDA(g, cub::DeviceSelect::Flagged(nullptr, bytes, in, flags, out, d_n, n, g->stream));
+    GIR_TRY(ensure(g, g->cub_tmp, bytes));
+    GIR_CUDA(g, cub::DeviceSelect::Flagged(g->cub_tmp.p, bytes, in, flags, out, d_n, n, g->stream));
+    void* h = nullptr;
+    GIR_TRY(pinned(g, 64, &h));
+    GIR_CUDA(g, cudaMemcpyAsync(h, d_n, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    *host_n = *static_cast<int64_t*>(h);
+    return GIR_OK;
+}
+
+int select_flagged_u64(gir_dev* g, const uint64_t* in, const uint8_t* flags, uint64_t* out, int64_t n, int64_t* host_n) {
+    return select_flagged(g, in, flags, out, n, host_n);
+}
+int select_flagged_i32(gir_dev* g, const int32_t* in, const uint8_t* flags, int32_t* out, int64_t n, int64_t* host_n) {
+    return select_flagged(g, in, flags, out, n, host_n);
+}
+int select_flagged_iota(gir_dev* g, const uint8_t* flags, int32_t* out, int64_t n, int64_t* host_n) {
+    return select_flagged(g, cub::CountingInputIterator<int32_t>(0), flags, out, n, host_n);
+}
+
+}  // namespace gir

@@ -1,0 +1,96 @@
+// Weakly connected components (buildWCC, gir_constructor/gir.cpp:593-655).
+//
+// The reference runs a sequential union-find over the forward edges (gir.cpp:635-653). Here
+// every edge is linked concurrently into a lock-free union-find forest: link(u, w) finds both
+// roots (with path halving) and hooks the larger root under the smaller one by compare-and-
+// swap, retrying when another thread moved the root first. A root is therefore always the
+// smallest vertex of its tree, and after a final pointer-jumping pass every vertex points at
+// the smallest vertex id of its component -- the canonical label.
+#include "common.cuh"
+
+namespace gir {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ int32_t uf_find(int32_t* parent, int32_t x) {
+    int32_t p = parent[x];
+    while (p != x) {
+        const int32_t gp = parent[p];
+        if (gp != p) parent[x] = gp;  // path halving (benign race: always an ancestor)
+        x = p;
+        p = parent[x];
+    }
+    return x;
+}
+
+// Lock-free: a failed CAS means another link moved rb first, so the retries are bounded by
+// the concurrent links; the cap only turns a broken invariant into an error status.
+__device__ __forceinline__ void uf_link(int32_t* parent, int32_t a, int32_t b, int32_t* err) {
+    for (int iter = 0; iter < (1 << 22); ++iter) {
+        int32_t ra = uf_find(parent, a), rb = uf_find(parent, b);
+        if (ra == rb) return;
+        if (ra > rb) { const int32_t t = ra; ra = rb; rb = t; }
+        if (atomicCAS(&parent[rb], rb, ra) == rb) return;
+    }
+    atomicExch(err, 1);
+}
+
+__global__ void k_uf_init(int32_t* parent, int64_t V) { GRID_STRIDE(v, V) parent[v] = (int32_t)v; }
+
+__global__ void __launch_bounds__(kBlock) k_uf_link_rows(CSRView c, int64_t V, int32_t* parent, int32_t* err) {
+    __shared__ int64_t s_excl[kBlock / 32][33];
+    __shared__ int32_t s_u[kBlock / 32][32];
+    const int wib = threadIdx.x >> 5;
+    warp_sweep_rows(c.beg, c.deg, c.adj, 0, V, s_excl[wib], s_u[wib],
+                    [&](int32_t u, int32_t w, int64_t) { uf_link(parent, u, w, err); });
+}
+
+__global__ void k_uf_compress(int32_t* parent, int64_t V, unsigned long long* roots) {
+    unsigned long long r = 0;
+    GRID_STRIDE(v, V) {
+        const int32_t x = uf_find(parent, (int32_t)v);
+        parent[v] = x;
+        r += (x == (int32_t)v);
+    }
+    for (int o = 16; o; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if ((threadIdx.x & 31) == 0 && r) atomicAdd(roots, r);
+}
+
+}  // namespace
+
+// Components of the undirected view of `c` (a forward CSR), labels = smallest vertex id.
+int wcc_labels(gir_dev* g, const DevCSR& c, int32_t* label, int64_t* n_comp) {
+    const int64_t V = g->V;
+    unsigned long long* roots = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[14], 4, &roots));
+    int32_t* err = reinterpret_cast<int32_t*>(roots + 1);
+    GIR_CUDA(g, cudaMemsetAsync(roots, 0, 2 * sizeof(unsigned long long), g->stream));
+    if (V == 0) { *n_comp = 0; return GIR_OK; }
+    k_uf_init<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(label, V);
+    GIR_LAUNCH(g, "k_uf_init");
+    k_uf_link_rows<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(view(c), V, label, err);
+    GIR_LAUNCH(g, "k_uf_link_rows");
+    k_uf_compress<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(label, V, roots);
+    GIR_LAUNCH(g, "k_uf_compress");
+    unsigned long long h[2] = {0, 0};
+    GIR_CUDA(g, cudaMemcpyAsync(h, roots, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    if (h[1]) return fail(g, GIR_ERR_TIMEOUT, "wcc: union-find link exceeded its retry bound");
+    *n_comp = (int64_t)h[0];
+    return GIR_OK;
+}
+
+int wcc_build(gir_dev* g) {
+    int32_t* label = nullptr;
+    GIR_TRY(ensure_n(g, g->wcc, g->V + 1, &label));
+    GIR_TRY(wcc_labels(g, g->fw, label, &g->n_wcc));
+    g->wcc_built = true;
+    return GIR_OK;
+}
+
+}  // namespace gir

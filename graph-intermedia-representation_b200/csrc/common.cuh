@@ -268,6 +268,52 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t* q
     base = __shfl_sync(0xffffffffu, base, leader);
     if (pred) q[base + __popc(m & ((1u << lane_id()) - 1))] = value;
 }
+
+// Frontier expansion over one CSR: a warp takes 32 queue entries and walks their rows together.
+// f(u, w) is called for every entry w of row u; it returns true when w joins the next queue.
+template <class F>
+__device__ __forceinline__ void warp_expand(const int32_t* q, int64_t n, const CSRView& c, int32_t* nq,
+                                            unsigned long long* ncnt, F&& f) {
+    constexpr int kW = 32;  // supports blocks of up to 1024 threads
+    __shared__ int64_t s_excl[kW][33];
+    __shared__ int32_t s_u[kW][32];
+    const int lane = lane_id(), wib = threadIdx.x >> 5;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
+        const int64_t i = base + lane;
+        const int32_t u = i < n ? q[i] : -1;
+        const int64_t cnt = u >= 0 ? c.deg[u] : 0;
+        int64_t incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        s_excl[wib][lane] = incl - cnt;
+        if (lane == 31) s_excl[wib][32] = incl;
+        s_u[wib][lane] = u;
+        __syncwarp();
+        const int64_t total = s_excl[wib][32];
+        for (int64_t p0 = 0; p0 < total; p0 += 32) {
+            const int64_t p = p0 + lane;
+            bool push = false;
+            int32_t w = 0;
+            if (p < total) {
+                int lo = 0, hi = 31;
+                while (lo < hi) {
+                    const int m = (lo + hi + 1) >> 1;
+                    if (s_excl[wib][m] <= p) lo = m; else hi = m - 1;
+                }
+                const int32_t uu = s_u[wib][lo];
+                w = c.adj[c.beg[uu] + (p - s_excl[wib][lo])];
+                push = f(uu, w);
+            }
+            warp_append(push, w, nq, ncnt);
+        }
+        __syncwarp();
+    }
+}
+
 #endif
 
 }  // namespace gir

@@ -1,6 +1,500 @@
-// Strongly connected components + condensation DAG (buildSCC_DAG, gir.cpp:798-839).
+// Strongly connected components and the condensation DAG (buildSCC_DAG, gir.cpp:798-839).
+//
+// The reference runs one sequential iterative Tarjan over all vertices (gir.cpp:494-537) and
+// counts cross-SCC edges into per-SCC hash maps (gir.cpp:825-831). The partition is unique,
+// so any exact algorithm gives the same SCCs; here it is the data-parallel decomposition
+// (as in iSpan / Multistep, gir_constructor/includes/scc_cpu):
+//  1. trim-1 as a worklist: a vertex without an in- or out-neighbour among the unassigned
+//     vertices (self-loops ignored) is a singleton SCC; removing it lowers its neighbours'
+//     counts, which may trim them in turn;
+//  2. forward-backward from a pivot of maximal out-degree x in-degree (the giant SCC of a
+//     power-law graph): SCC(pivot) = forward reach ∩ backward reach over unassigned vertices;
+//  3. colour propagation for the rest, repeated until every vertex is assigned: every
+//     unassigned vertex starts with its own id as colour, colours spread along forward edges
+//     by max until stable, so colour(v) = largest id that reaches v; a vertex r with
+//     colour(r) = r is a root, and SCC(r) = the vertices of colour r that reach r (a backward
+//     search restricted to colour r);
+//  4. labels are made canonical (smallest member id) and the condensation edges are the
+//     distinct (scc(u), scc(v)) keys of all cross edges: radix sort + unique;
+//  5. topological ranks: Kahn levels over the condensation DAG, rank = position in
+//     (level, label) order, so rank(a) < rank(b) for every DAG edge a -> b (the invariant of
+//     scc_rank, gir.h:54-57).
 #include "common.cuh"
 
 namespace gir {
-int scc_build(gir_dev* g) { return fail(g, GIR_ERR_STATE, "buildSCC_DAG: not available in this build"); }
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kWarps = kBlock / 32;
+
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+enum { C_Q = 0, C_ACT = 1, C_ROOTS = 2, C_PIV = 3, C_N = 8 };
+
+// Active in/out degree counts (self-loops excluded) and the first trim frontier.
+__global__ void k_trim_init(int64_t V, CSRView fw, CSRView bw, int32_t* label, int32_t* indeg, int32_t* outdeg,
+                            int32_t* q, unsigned long long* cnt) {
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = base + threadIdx.x;
+        bool trim = false;
+        if (v < V) {
+            int32_t o = fw.deg[v], in = bw.deg[v];
+            // self-loop: rows are sorted, binary search for v
+            const int64_t fb = fw.beg[v];
+            const int64_t p = lower_bound_dev(fw.adj, fb, fb + o, (int32_t)v);
+            if (p < fb + o && fw.adj[p] == (int32_t)v) { --o; --in; }
+            outdeg[v] = o;
+            indeg[v] = in;
+            trim = (o == 0 || in == 0);
+            label[v] = trim ? (int32_t)v : -1;
+        }
+        warp_append(trim, (int32_t)v, q, &cnt[C_Q]);
+    }
+}
+
+// One trim round over the removed vertices of the last round: lower the counts of their
+// neighbours; a neighbour whose count reaches 0 is removed (claimed once by CAS).
+__global__ void __launch_bounds__(kBlock) k_trim_out(const int32_t* q, const unsigned long long* qlen, CSRView fw,
+                                                     int32_t* label, int32_t* indeg, int32_t* nq,
+                                                     unsigned long long* cnt) {
+    warp_expand(q, (int64_t)*qlen, fw, nq, &cnt[C_Q], [&](int32_t u, int32_t w) {
+        if (w == u) return false;
+        if (atomicSub(&indeg[w], 1) == 1) return atomicCAS(&label[w], -1, w) == -1;
+        return false;
+    });
+}
+
+__global__ void __launch_bounds__(kBlock) k_trim_in(const int32_t* q, const unsigned long long* qlen, CSRView bw,
+                                                    int32_t* label, int32_t* outdeg, int32_t* nq,
+                                                    unsigned long long* cnt) {
+    warp_expand(q, (int64_t)*qlen, bw, nq, &cnt[C_Q], [&](int32_t u, int32_t w) {
+        if (w == u) return false;
+        if (atomicSub(&outdeg[w], 1) == 1) return atomicCAS(&label[w], -1, w) == -1;
+        return false;
+    });
+}
+
+// Pivot: the unassigned vertex with the largest out x in degree (ties: larger id).
+__global__ void k_pivot(int64_t V, const int32_t* label, const int32_t* indeg, const int32_t* outdeg,
+                        unsigned long long* cnt) {
+    unsigned long long best = 0;
+    unsigned long long act = 0;
+    GRID_STRIDE(v, V) {
+        if (label[v] != -1) continue;
+        ++act;
+        const unsigned long long s = (unsigned long long)(uint32_t)outdeg[v] * (unsigned long long)(uint32_t)indeg[v];
+        const unsigned long long k = ((s < (1ull << 31) ? s : (1ull << 31)) << 32) | (unsigned long long)v;
+        if (k + 1 > best) best = k + 1;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+        best = t > best ? t : best;
+        act += __shfl_xor_sync(0xffffffffu, act, o);
+    }
+    if (lane_id() == 0) {
+        if (best) atomicMax(&cnt[C_PIV], best);
+        if (act) atomicAdd(&cnt[C_ACT], act);
+    }
+}
+
+// Reach over unassigned vertices whose mark is not `epoch` yet (marks them).
+__global__ void __launch_bounds__(kBlock) k_reach(const int32_t* q, const unsigned long long* qlen, CSRView c,
+                                                  const int32_t* label, int32_t* mark, int32_t epoch, int32_t* nq,
+                                                  unsigned long long* cnt) {
+    warp_expand(q, (int64_t)*qlen, c, nq, &cnt[C_Q], [&](int32_t, int32_t w) {
+        if (label[w] != -1 || mark[w] == epoch) return false;
+        return atomicExch(&mark[w], epoch) != epoch;
+    });
+}
+
+// Backward reach from the pivot over unassigned vertices that the forward reach marked:
+// they form SCC(pivot) and get its label.
+__global__ void __launch_bounds__(kBlock) k_reach_bw_in_fw(const int32_t* q, const unsigned long long* qlen, CSRView bw,
+                                                           int32_t* label, const int32_t* mark, int32_t epoch,
+                                                           int32_t pivot, int32_t* nq, unsigned long long* cnt) {
+    warp_expand(q, (int64_t)*qlen, bw, nq, &cnt[C_Q], [&](int32_t, int32_t w) {
+        if (mark[w] != epoch) return false;
+        return atomicCAS(&label[w], -1, pivot) == -1;
+    });
+}
+
+// Colour propagation: colour(w) = max(colour(w), colour(u)) along forward edges between
+// unassigned vertices. `inq` de-duplicates the next queue per round.
+__global__ void k_color_init(int64_t V, const int32_t* label, int32_t* color, int32_t* q, unsigned long long* cnt) {
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = base + threadIdx.x;
+        const bool on = v < V && label[v] == -1;
+        if (v < V) color[v] = (int32_t)v;
+        warp_append(on, (int32_t)v, q, &cnt[C_Q]);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_color_prop(const int32_t* q, const unsigned long long* qlen, CSRView fw,
+                                                       const int32_t* label, int32_t* color, int32_t* inq,
+                                                       int32_t round, int32_t* nq, unsigned long long* cnt) {
+    warp_expand(q, (int64_t)*qlen, fw, nq, &cnt[C_Q], [&](int32_t u, int32_t w) {
+        if (label[w] != -1) return false;
+        const int32_t cu = color[u];
+        if (cu <= color[w]) return false;
+        if (atomicMax(&color[w], cu) >= cu) return false;
+        return atomicExch(&inq[w], round) != round;
+    });
+}
+
+__global__ void k_color_roots(int64_t V, int32_t* label, const int32_t* color, int32_t* q, unsigned long long* cnt) {
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = base + threadIdx.x;
+        bool root = false;
+        if (v < V && label[v] == -1 && color[v] == (int32_t)v) {
+            label[v] = (int32_t)v;
+            root = true;
+        }
+        warp_append(root, (int32_t)v, q, &cnt[C_Q]);
+    }
+}
+
+// Backward search inside each colour class from its root.
+__global__ void __launch_bounds__(kBlock) k_color_bw(const int32_t* q, const unsigned long long* qlen, CSRView bw,
+                                                     int32_t* label, const int32_t* color, int32_t* nq,
+                                                     unsigned long long* cnt) {
+    warp_expand(q, (int64_t)*qlen, bw, nq, &cnt[C_Q], [&](int32_t u, int32_t w) {
+        const int32_t c = color[u];
+        if (label[w] != -1 || color[w] != c) return false;
+        return atomicCAS(&label[w], -1, c) == -1;
+    });
+}
+
+// Canonical labels: smallest member of every class.
+__global__ void k_fill(int32_t* p, int64_t n, int32_t v) { GRID_STRIDE(i, n) p[i] = v; }
+
+__global__ void k_class_min(int64_t V, const int32_t* label, int32_t* mn) {
+    GRID_STRIDE(v, V) atomicMin(&mn[label[v]], (int32_t)v);
+}
+
+__global__ void k_apply_min(int64_t V, int32_t* label, const int32_t* mn, unsigned long long* n_classes) {
+    unsigned long long c = 0;
+    GRID_STRIDE(v, V) {
+        const int32_t m = mn[label[v]];
+        label[v] = m;
+        c += (m == (int32_t)v);
+    }
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane_id() == 0 && c) atomicAdd(n_classes, c);
+}
+
+// Cross-SCC edge keys (label(u) << 32 | label(w)) at the edge's own slot, flagged; the flags of
+// slack slots stay 0 (cleared by the caller), so a compaction over the capacity collects them.
+__global__ void __launch_bounds__(kBlock) k_cross_keys(int64_t V, CSRView fw, const int32_t* label, uint64_t* keys,
+                                                       uint8_t* flag) {
+    __shared__ int64_t s_excl[kWarps][33];
+    __shared__ int32_t s_u[kWarps][32];
+    const int wib = threadIdx.x >> 5;
+    warp_sweep_rows(fw.beg, fw.deg, fw.adj, 0, V, s_excl[wib], s_u[wib], [&](int32_t u, int32_t w, int64_t e) {
+        const int32_t a = label[u], b = label[w];
+        keys[e] = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
+        flag[e] = a != b;
+    });
+}
+
+__global__ void k_dag_dst(const uint64_t* keys, int64_t n, int32_t* dst) {
+    GRID_STRIDE(i, n) dst[i] = (int32_t)(keys[i] & 0xffffffffULL);
+}
+
+__global__ void k_distinct_u64(const uint64_t* keys, int64_t n, uint8_t* flag) {
+    GRID_STRIDE(i, n) flag[i] = (i == 0 || keys[i] != keys[i - 1]);
+}
+
+// ---- topological levels over the condensation DAG (rows: keys sorted by source label) ----
+__global__ void k_dag_indeg(const uint64_t* keys, int64_t n, int32_t* indeg) {
+    GRID_STRIDE(i, n) atomicAdd(&indeg[(int64_t)(keys[i] & 0xffffffffULL)], 1);
+}
+
+__global__ void k_dag_rows(const uint64_t* keys, int64_t n, int64_t* first, int32_t* cnt) {
+    GRID_STRIDE(i, n) {
+        const int64_t a = (int64_t)(keys[i] >> 32);
+        if (i == 0 || (int64_t)(keys[i - 1] >> 32) != a) first[a] = i;
+        atomicAdd(&cnt[a], 1);
+    }
+}
+
+__global__ void k_dag_sources(int64_t V, const int32_t* label, const int32_t* indeg, int32_t* level, int32_t* q,
+                              unsigned long long* cnt) {
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = base + threadIdx.x;
+        bool src = false;
+        if (v < V && label[v] == (int32_t)v) {
+            if (indeg[v] == 0) { src = true; level[v] = 0; }
+        }
+        warp_append(src, (int32_t)v, q, &cnt[C_Q]);
+    }
+}
+
+// One Kahn round: DAG nodes of the queue release their out-edges (rows: first / rcnt / dst).
+__global__ void __launch_bounds__(kBlock) k_dag_step(const int32_t* q, const unsigned long long* qlen, CSRView dagc,
+                                                     int32_t* indeg, int32_t* level, int32_t L, int32_t* nq,
+                                                     unsigned long long* cnt) {
+    warp_expand(q, (int64_t)*qlen, dagc, nq, &cnt[C_Q], [&](int32_t, int32_t b) {
+        if (atomicSub(&indeg[b], 1) != 1) return false;
+        level[b] = L + 1;
+        return true;
+    });
+}
+
+__global__ void k_rank_keys(int64_t V, const int32_t* label, const int32_t* level, uint64_t* keys,
+                            unsigned long long* n) {
+    GRID_STRIDE(v, V) {
+        if (label[v] == (int32_t)v) keys[atomicAdd(n, 1ull)] = ((uint64_t)(uint32_t)level[v] << 32) | (uint32_t)v;
+    }
+}
+
+__global__ void k_rank_scatter(const uint64_t* keys, int64_t n, int32_t* rank_of) {
+    GRID_STRIDE(i, n) rank_of[(int64_t)(keys[i] & 0xffffffffULL)] = (int32_t)i;
+}
+
+__global__ void k_rank_gather(int64_t V, const int32_t* label, const int32_t* rank_of, int32_t* rank) {
+    GRID_STRIDE(v, V) rank[v] = rank_of[label[v]];
+}
+
+struct Loop {
+    gir_dev* g;
+    unsigned long long* cnt;
+    unsigned long long* hc;
+    int read(int64_t* out) {
+        GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+        *out = (int64_t)hc[C_Q];
+        return GIR_OK;
+    }
+};
+
+}  // namespace
+
+int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
+    const int64_t V = g->V;
+    const CSRView fw = view(g->fw), bw = view(g->bw);
+    int32_t *indeg = nullptr, *outdeg = nullptr, *qa = nullptr, *qb = nullptr, *mark = nullptr, *color = nullptr;
+    unsigned long long* cnt = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &indeg));
+    GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &outdeg));
+    GIR_TRY(ensure_n(g, g->scratch[2], V + 1, &qa));
+    GIR_TRY(ensure_n(g, g->scratch[3], V + 1, &qb));
+    GIR_TRY(ensure_n(g, g->scratch[4], V + 1, &mark));
+    GIR_TRY(ensure_n(g, g->scratch[5], V + 1, &color));
+    GIR_TRY(ensure_n(g, g->scratch[6], 2 * C_N, &cnt));
+    unsigned long long* qlen = cnt + C_N;
+    void* hp = nullptr;
+    GIR_TRY(pinned(g, 256, &hp));
+    Loop lp{g, cnt, static_cast<unsigned long long*>(hp)};
+    *n_scc = 0;
+    if (V == 0) return GIR_OK;
+    const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
+    auto blocks_for_queue = [&](int64_t n) {
+        const int64_t b = (n + 32 * kWarps - 1) / (32 * kWarps);
+        return (int)(b < 1 ? 1 : (b < grid ? b : grid));
+    };
+    // One level-synchronous pass: `launch(in, inlen, out)` for each round until the queue empties.
+    auto run_queue = [&](int32_t*& in, int32_t*& out, int64_t n, auto&& launch) -> int {
+        while (n > 0) {
+            GIR_CUDA(g, cudaMemcpyAsync(qlen, &cnt[C_Q], sizeof(unsigned long long), cudaMemcpyDeviceToDevice, g->stream));
+            GIR_CUDA(g, cudaMemsetAsync(&cnt[C_Q], 0, sizeof(unsigned long long), g->stream));
+            GIR_TRY(launch(in, out, n));
+            std::swap(in, out);
+            GIR_TRY(lp.read(&n));
+        }
+        return GIR_OK;
+    };
+
+    // 1. trim-1
+    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 2 * C_N, g->stream));
+    k_trim_init<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, fw, bw, label, indeg, outdeg, qa, cnt);
+    GIR_LAUNCH(g, "k_trim_init");
+    int64_t n = 0;
+    GIR_TRY(lp.read(&n));
+    GIR_TRY(run_queue(qa, qb, n, [&](int32_t* in, int32_t* out, int64_t m) -> int {
+        // removed vertices lower both neighbour counts; both kernels append to `out`
+        k_trim_out<<<blocks_for_queue(m), kBlock, 0, g->stream>>>(in, qlen, fw, label, indeg, out, cnt);
+        GIR_LAUNCH(g, "k_trim_out");
+        k_trim_in<<<blocks_for_queue(m), kBlock, 0, g->stream>>>(in, qlen, bw, label, outdeg, out, cnt);
+        GIR_LAUNCH(g, "k_trim_in");
+        return GIR_OK;
+    }));
+
+    // 2. forward-backward from the max-degree pivot
+    GIR_CUDA(g, cudaMemsetAsync(mark, 0, sizeof(int32_t) * V, g->stream));
+    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+    k_pivot<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, indeg, outdeg, cnt);
+    GIR_LAUNCH(g, "k_pivot");
+    GIR_CUDA(g, cudaMemcpyAsync(lp.hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    if (lp.hc[C_PIV] != 0) {
+        const int32_t pivot = (int32_t)((lp.hc[C_PIV] - 1) & 0xffffffffULL);
+        const int32_t epoch = 1;
+        // forward reach (marks), seeded with the pivot
+        GIR_CUDA(g, cudaMemcpyAsync(mark + pivot, &epoch, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
+        GIR_CUDA(g, cudaMemcpyAsync(qa, &pivot, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
+        const unsigned long long one = 1;
+        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+        GIR_CUDA(g, cudaMemcpyAsync(&cnt[C_Q], &one, sizeof(one), cudaMemcpyHostToDevice, g->stream));
+        GIR_TRY(run_queue(qa, qb, 1, [&](int32_t* in, int32_t* out, int64_t m) -> int {
+            k_reach<<<blocks_for_queue(m), kBlock, 0, g->stream>>>(in, qlen, fw, label, mark, epoch, out, cnt);
+            GIR_LAUNCH(g, "k_reach");
+            return GIR_OK;
+        }));
+        // backward reach inside the forward set: SCC(pivot)
+        GIR_CUDA(g, cudaMemcpyAsync(label + pivot, &pivot, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
+        GIR_CUDA(g, cudaMemcpyAsync(qa, &pivot, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
+        GIR_CUDA(g, cudaMemcpyAsync(&cnt[C_Q], &one, sizeof(one), cudaMemcpyHostToDevice, g->stream));
+        GIR_TRY(run_queue(qa, qb, 1, [&](int32_t* in, int32_t* out, int64_t m) -> int {
+            k_reach_bw_in_fw<<<blocks_for_queue(m), kBlock, 0, g->stream>>>(in, qlen, bw, label, mark, epoch, pivot,
+                                                                            out, cnt);
+            GIR_LAUNCH(g, "k_reach_bw_in_fw");
+            return GIR_OK;
+        }));
+    }
+
+    // 3. colour propagation rounds until every vertex is assigned
+    int32_t* inq = mark;
+    int32_t round = 1;
+    GIR_CUDA(g, cudaMemsetAsync(inq, 0, sizeof(int32_t) * V, g->stream));
+    for (int outer = 0; outer < (1 << 30); ++outer) {
+        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+        k_color_init<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, color, qa, cnt);
+        GIR_LAUNCH(g, "k_color_init");
+        GIR_TRY(lp.read(&n));
+        if (n == 0) break;
+        GIR_TRY(run_queue(qa, qb, n, [&](int32_t* in, int32_t* out, int64_t m) -> int {
+            ++round;
+            k_color_prop<<<blocks_for_queue(m), kBlock, 0, g->stream>>>(in, qlen, fw, label, color, inq, round, out, cnt);
+            GIR_LAUNCH(g, "k_color_prop");
+            return GIR_OK;
+        }));
+        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+        k_color_roots<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, color, qa, cnt);
+        GIR_LAUNCH(g, "k_color_roots");
+        GIR_TRY(lp.read(&n));
+        GIR_TRY(run_queue(qa, qb, n, [&](int32_t* in, int32_t* out, int64_t m) -> int {
+            k_color_bw<<<blocks_for_queue(m), kBlock, 0, g->stream>>>(in, qlen, bw, label, color, out, cnt);
+            GIR_LAUNCH(g, "k_color_bw");
+            return GIR_OK;
+        }));
+    }
+
+    // 4. canonical labels
+    int32_t* mn = color;
+    k_fill<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(mn, V, INT32_MAX);
+    GIR_LAUNCH(g, "k_fill");
+    k_class_min<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, mn);
+    GIR_LAUNCH(g, "k_class_min");
+    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+    k_apply_min<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, mn, &cnt[C_Q]);
+    GIR_LAUNCH(g, "k_apply_min");
+    GIR_TRY(lp.read(n_scc));
+    return GIR_OK;
+}
+
+int scc_build(gir_dev* g) {
+    const int64_t V = g->V;
+    int32_t* label = nullptr;
+    GIR_TRY(ensure_n(g, g->scc, V + 1, &label));
+    GIR_TRY(scc_labels(g, label, &g->n_scc));
+
+    // condensation edges: cross keys, radix sort, unique
+    const int64_t cap = g->fw.cap;
+    uint64_t *keys = nullptr, *tmp = nullptr;
+    uint8_t* flag = nullptr;
+    unsigned long long* cnt = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[7], cap + 1, &keys));
+    GIR_TRY(ensure_n(g, g->scratch[8], cap + 1, &tmp));
+    GIR_TRY(ensure_n(g, g->scratch[9], cap + 1, &flag));
+    GIR_TRY(ensure_n(g, g->scratch[6], 2 * C_N, &cnt));
+    void* hp = nullptr;
+    GIR_TRY(pinned(g, 256, &hp));
+    unsigned long long* hc = static_cast<unsigned long long*>(hp);
+    GIR_CUDA(g, cudaMemsetAsync(flag, 0, cap + 1, g->stream));
+    if (V > 0) {
+        k_cross_keys<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, view(g->fw), label, keys, flag);
+        GIR_LAUNCH(g, "k_cross_keys");
+    }
+    int64_t n_cross = 0;
+    GIR_TRY(select_flagged_u64(g, keys, flag, tmp, cap, &n_cross));
+    std::swap(keys, tmp);
+    GIR_TRY(sort_keys_u64(g, keys, tmp, n_cross, 64));
+    int64_t n_dag = 0;
+    uint64_t* dag = nullptr;
+    GIR_TRY(ensure_n(g, g->dag, n_cross + 1, &dag));
+    if (n_cross > 0) {
+        k_distinct_u64<<<grid_for(g, n_cross, kBlock), kBlock, 0, g->stream>>>(keys, n_cross, flag);
+        GIR_LAUNCH(g, "k_distinct_u64");
+        GIR_TRY(select_flagged_u64(g, keys, flag, dag, n_cross, &n_dag));
+    }
+    g->n_dag = n_dag;
+
+    // topological ranks by Kahn levels
+    int32_t *indeg = nullptr, *level = nullptr, *qa = nullptr, *qb = nullptr, *rcnt = nullptr, *rank_of = nullptr;
+    int64_t* first = nullptr;
+    int32_t *rank = nullptr, *dst = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[11], n_dag + 1, &dst));
+    GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &indeg));
+    GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &level));
+    GIR_TRY(ensure_n(g, g->scratch[2], V + 1, &qa));
+    GIR_TRY(ensure_n(g, g->scratch[3], V + 1, &qb));
+    GIR_TRY(ensure_n(g, g->scratch[4], V + 1, &rcnt));
+    GIR_TRY(ensure_n(g, g->scratch[5], V + 1, &rank_of));
+    GIR_TRY(ensure_n(g, g->scratch[10], V + 1, &first));
+    GIR_TRY(ensure_n(g, g->scc_rank, V + 1, &rank));
+    GIR_CUDA(g, cudaMemsetAsync(indeg, 0, sizeof(int32_t) * V, g->stream));
+    GIR_CUDA(g, cudaMemsetAsync(rcnt, 0, sizeof(int32_t) * V, g->stream));
+    GIR_CUDA(g, cudaMemsetAsync(level, 0, sizeof(int32_t) * V, g->stream));
+    if (n_dag > 0) {
+        k_dag_indeg<<<grid_for(g, n_dag, kBlock), kBlock, 0, g->stream>>>(dag, n_dag, indeg);
+        GIR_LAUNCH(g, "k_dag_indeg");
+        k_dag_rows<<<grid_for(g, n_dag, kBlock), kBlock, 0, g->stream>>>(dag, n_dag, first, rcnt);
+        GIR_LAUNCH(g, "k_dag_rows");
+        k_dag_dst<<<grid_for(g, n_dag, kBlock), kBlock, 0, g->stream>>>(dag, n_dag, dst);
+        GIR_LAUNCH(g, "k_dag_dst");
+    }
+    const CSRView dagc{first, rcnt, dst, nullptr};
+    unsigned long long* qlen = cnt + C_N;
+    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+    if (V > 0) {
+        k_dag_sources<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, indeg, level, qa, cnt);
+        GIR_LAUNCH(g, "k_dag_sources");
+    }
+    GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    int64_t nq = (int64_t)hc[C_Q];
+    int32_t L = 0;
+    while (nq > 0) {
+        GIR_CUDA(g, cudaMemcpyAsync(qlen, &cnt[C_Q], sizeof(unsigned long long), cudaMemcpyDeviceToDevice, g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(&cnt[C_Q], 0, sizeof(unsigned long long), g->stream));
+        k_dag_step<<<grid_for(g, nq * 32, kBlock), kBlock, 0, g->stream>>>(qa, qlen, dagc, indeg, level, L, qb, cnt);
+        GIR_LAUNCH(g, "k_dag_step");
+        std::swap(qa, qb);
+        GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+        nq = (int64_t)hc[C_Q];
+        ++L;
+    }
+    // rank = position in (level, label) order
+    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+    if (V > 0) {
+        k_rank_keys<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, level, keys, &cnt[C_Q]);
+        GIR_LAUNCH(g, "k_rank_keys");
+    }
+    GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    const int64_t ns = (int64_t)hc[C_Q];
+    GIR_TRY(sort_keys_u64(g, keys, tmp, ns, 64));
+    if (ns > 0) {
+        k_rank_scatter<<<grid_for(g, ns, kBlock), kBlock, 0, g->stream>>>(keys, ns, rank_of);
+        GIR_LAUNCH(g, "k_rank_scatter");
+        k_rank_gather<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, rank_of, rank);
+        GIR_LAUNCH(g, "k_rank_gather");
+    }
+    g->scc_built = true;
+    return GIR_OK;
+}
+
 }  // namespace gir

@@ -50,10 +50,13 @@ __global__ void __launch_bounds__(kBlock) k_uf_link_rows(CSRView c, int64_t V, i
                     [&](int32_t u, int32_t w, int64_t) { uf_link(parent, u, w, err); });
 }
 
+// Final pointer jumping. The walk only reads: with path halving, another thread could replace
+// a root just stored in parent[v] by an intermediate ancestor; here every write is a final root.
 __global__ void k_uf_compress(int32_t* parent, int64_t V, unsigned long long* roots) {
     unsigned long long r = 0;
     GRID_STRIDE(v, V) {
-        const int32_t x = uf_find(parent, (int32_t)v);
+        int32_t x = (int32_t)v;
+        while (parent[x] != x) x = parent[x];
         parent[v] = x;
         r += (x == (int32_t)v);
     }

@@ -1,0 +1,171 @@
+"""GPU parity of the structural layers (buildWCC / buildSCC_DAG / buildBCT and their upkeep under
+updates) through the C ABI: canonical WCC and SCC partitions, condensation-DAG edge sets, blocks
+and articulation points, bit-exact against the reference's golden vectors after every update
+step and against the oracle on R-MAT graphs."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _layers(pkg, orc, d):
+    n = pkg.native
+    scc = d.labels(n.LABEL_SCC)
+    src, dst = d.dag()
+    dag = (src.astype(np.int64) << 32) | dst.astype(np.int64)
+    label, head = d.blocks()
+    blocks = orc.canon_blocks_from_device(label, head)
+    ap = d.labels(n.LABEL_BCNT) >= 2
+    return d.labels(n.LABEL_WCC), scc, dag, blocks, ap
+
+
+def _check_ranks(pkg, d):
+    scc = d.labels(pkg.native.LABEL_SCC)
+    rank = d.labels(pkg.native.LABEL_SCC_RANK)
+    src, dst = d.dag()
+    # rank is per SCC and respects every condensation edge (gir.h:54-57)
+    assert np.all(rank == rank[scc])
+    assert np.all(rank[src] < rank[dst])
+    reps = np.nonzero(scc == np.arange(len(scc)))[0]
+    assert len(np.unique(rank[reps])) == len(reps)
+
+
+def _check_block_invariants(pkg, d):
+    """checkBlockForestInvariants (gir.cpp:4159-4211), in this representation: every block has
+    at least one vertex whose parent block it is, heads of non-root blocks are APs, and the
+    count array matches the memberships."""
+    label, head = d.blocks()
+    bcnt = d.labels(pkg.native.LABEL_BCNT)
+    V = len(label)
+    assert label.min(initial=0) >= 0 and (V == 0 or label.max() < len(head))
+    counts = np.bincount(label, minlength=len(head))
+    assert np.all(counts >= 1)
+    exp = np.ones(V, np.int64)
+    np.add.at(exp, head[head >= 0], 1)
+    np.testing.assert_array_equal(bcnt, exp)
+    assert np.all(bcnt[head[head >= 0]] >= 2)
+
+
+def _match(pkg, orc, d, golden, key):
+    wcc, scc, dag, blocks, ap = _layers(pkg, orc, d)
+    np.testing.assert_array_equal(wcc, golden[f"{key}/wcc"], err_msg=f"{key} wcc")
+    np.testing.assert_array_equal(scc, golden[f"{key}/scc"], err_msg=f"{key} scc")
+    np.testing.assert_array_equal(dag, golden[f"{key}/dag"], err_msg=f"{key} dag")
+    np.testing.assert_array_equal(blocks, golden[f"{key}/blocks"], err_msg=f"{key} blocks")
+    np.testing.assert_array_equal(ap, golden[f"{key}/ap"], err_msg=f"{key} ap")
+    _check_ranks(pkg, d)
+    _check_block_invariants(pkg, d)
+
+
+def test_golden_layers_after_every_step(pkg, orc, golden):
+    for case in golden_cases(golden):
+        V = int(golden[f"{case}/V"][0])
+        d = pkg.DeviceGraph.create(golden[f"{case}/in_fw_beg"], golden[f"{case}/in_fw_adj"],
+                                   golden[f"{case}/in_bw_beg"], golden[f"{case}/in_bw_adj"], V)
+        d.build(pkg.native.LAYER_ALL)
+        _match(pkg, orc, d, golden, f"{case}/s0")
+        for k in range(1, int(golden[f"{case}/steps"][0]) + 1):
+            key = f"{case}/s{k}"
+            d.apply_batch(golden[f"{key}/ops_u"], golden[f"{key}/ops_v"], golden[f"{key}/ops_ins"])
+            _match(pkg, orc, d, golden, key)
+        d.close()
+
+
+def test_call_order_enforced(pkg, golden):
+    case = "example"
+    d = pkg.DeviceGraph.create(golden[f"{case}/in_fw_beg"], golden[f"{case}/in_fw_adj"],
+                               golden[f"{case}/in_bw_beg"], golden[f"{case}/in_bw_adj"], 18)
+    with pytest.raises(pkg.GirError) as e:
+        d.build(pkg.native.LAYER_BCT)
+    assert e.value.code == 6
+    with pytest.raises(pkg.GirError):
+        d.labels(pkg.native.LABEL_SCC)
+    d.close()
+
+
+def test_gir_class_surface(pkg, golden):
+    """The reference surface (getNodeToScc, getDAG, getBCTComponents, ...) on the example graph."""
+    case = "example"
+    g = pkg.graphs.Graph(18, golden[f"{case}/in_fw_beg"], golden[f"{case}/in_fw_adj"],
+                         golden[f"{case}/in_bw_beg"], golden[f"{case}/in_bw_adj"])
+    G = pkg.GIR(graph=g)
+    G.buildWCC(); G.buildSCC_DAG(); G.buildBCT()
+    n2s = G.getNodeToScc()
+    assert n2s[0] == n2s[9] and n2s[0] != n2s[12]
+    wccs_before = len(G.getWCCs())
+    G.insertEdge(3, 12)
+    assert len(G.getWCCs()) == wccs_before - 1
+    G.deleteEdge(3, 12)
+    assert len(G.getWCCs()) == wccs_before
+    G.updateEdgeUndirected(9, 2, False)  # routes as directed 9->2 (gir.cpp:3134)
+    n2s = G.getNodeToScc()
+    assert n2s[0] != n2s[9] and n2s[9] == n2s[10] == n2s[11]
+    dag = G.getDAG()
+    assert any(dag[r] for r in range(18))
+    comps = G.getBCTComponents(G.sccOf(0))
+    assert sorted(map(sorted, comps)) == sorted(map(sorted, [[0, 1, 2]]))
+    assert G.hasDirectedEdge(2, 9) and not G.hasDirectedEdge(9, 2) and G.hasUndirectedEdge(9, 2)
+    assert G.bfs(0)[9] == 3  # 0 -> 1 -> 2 -> 9
+    assert G.sssp(0)[0] == 0 and G.sssp(0)[1] == G.edgeWeight(0, 1)
+
+
+@pytest.fixture(scope="module")
+def s16(pkg, orc):
+    g = pkg.graphs.rmat_s16()
+    fb, fa = orc.normalize(g.V, g.fw_beg, g.fw_adj)
+    return g, fb, fa
+
+
+def _oracle_match(pkg, orc, d, V, fb, fa, what):
+    L = orc.Layers(V, fb, fa)
+    wcc, scc, dag, blocks, ap = _layers(pkg, orc, d)
+    np.testing.assert_array_equal(wcc, L.wcc, err_msg=f"{what} wcc")
+    np.testing.assert_array_equal(scc, L.scc, err_msg=f"{what} scc")
+    np.testing.assert_array_equal(dag, L.dag, err_msg=f"{what} dag")
+    np.testing.assert_array_equal(blocks, L.blocks, err_msg=f"{what} blocks")
+    np.testing.assert_array_equal(ap, L.ap, err_msg=f"{what} ap")
+    _check_ranks(pkg, d)
+    _check_block_invariants(pkg, d)
+
+
+def test_rmat_s16_layers_and_batches(pkg, orc, s16):
+    g, fb, fa = s16
+    d = pkg.DeviceGraph.from_graph(g)
+    d.build(pkg.native.LAYER_ALL)
+    _oracle_match(pkg, orc, d, g.V, fb, fa, "build")
+    for step, (ni, nd) in enumerate(((1000, 0), (0, 1000), (20000, 20000))):
+        cb, ca = d.csr(0)
+        gg = pkg.graphs.Graph(g.V, cb.astype(np.int32), ca, None, None)
+        u, v, ins = pkg.graphs.updates(gg, ni, nd, 200 + step)
+        d.apply_batch(u, v, ins)
+        fb, fa, _, _ = orc.apply_batch(g.V, fb, fa, u, v, ins)
+        _oracle_match(pkg, orc, d, g.V, fb, fa, f"batch {step}")
+    d.close()
+
+
+def test_shapes_high_diameter_and_dense(pkg, orc):
+    """A long directed cycle (one SCC, deep BFS tree, no AP), a path of 2-cycles (every inner
+    vertex an AP), a lattice (symmetric, many blocks) and a dense random graph."""
+    cases = []
+    n = 3000
+    cases.append(("cycle", n, np.arange(n), (np.arange(n) + 1) % n))
+    m = 2000
+    a = np.arange(m - 1)
+    cases.append(("path2", m, np.concatenate([a, a + 1]), np.concatenate([a + 1, a])))
+    lat = pkg.graphs.lattice(side=40, seed=8)
+    rows = np.repeat(np.arange(lat.V), np.diff(lat.fw_beg))
+    cases.append(("lattice", lat.V, rows, lat.fw_adj))
+    rng = np.random.default_rng(5)
+    cases.append(("dense", 500, rng.integers(0, 500, 20000), rng.integers(0, 500, 20000)))
+    for name, V, s, t in cases:
+        s = np.asarray(s, np.int32)
+        t = np.asarray(t, np.int32)
+        keep = s != t
+        gg = pkg.graphs.from_edges(V, s[keep], t[keep])
+        d = pkg.DeviceGraph.from_graph(gg, weights=False)
+        d.build(pkg.native.LAYER_ALL)
+        fb, fa = orc.normalize(V, gg.fw_beg, gg.fw_adj)
+        _oracle_match(pkg, orc, d, V, fb, fa, name)
+        d.close()

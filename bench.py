@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""GIR-B200 benchmark: BFS / SSSP GTEPS and update throughput on one B200 (or N replicas).
+
+One step = 64 BFS queries + 64 SSSP queries (Delta-stepping, Delta = 16, the reference's
+GIR::edgeWeight weights in [1, 100], so the reference computes the identical result) on the
+4.8M-vertex / 69M-edge power-law R-MAT graph (ids permuted, seed 3; a seeded synthetic stand-in
+for soc-LiveJournal1). GTEPS = traversed edges (out-edges of the reached vertices, summed over the
+queries) / time. The graph (~1.6 GB in HBM) is larger than L2, so no L2 flush is needed.
+
+  value      device-resident run: sources and result buffers already in HBM
+  e2e        the same calls through the C ABI with pinned HOST buffers: the sources are copied in
+             and the 64 level rows + 64 distance rows copied out inside every step
+  roofline   the dominant kernel's algorithmic bytes / its CUDA-event time (live), against the
+             measured HBM copy bandwidth of this pool (MEASURED_PEAKS.json)
+  cpu_baseline  the reference GIR compiled from its own sources (oracle/_ref), timed on this
+             host's cores on a bounded sample of the same queries
+
+Also reported (not part of `value`): SSSP with the stored U[1,255] weights, the layer builds and
+update batches of 10K / 100K / 1M edges at 50/50 with every layer kept exact.
+
+Multi-GPU (torchrun): replicas -- every rank holds the whole graph and runs its own 64 + 64
+queries (weak scaling); the time is the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BFS/SSSP GTEPS, updates/s on 1 B200; learned vs fixed schedule, bit-exact"
+N_BFS = 64
+N_SSSP = 64
+DELTA = 16
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="rmat_lj", choices=["rmat_lj", "rmat_s16"])
+    p.add_argument("--no-updates", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def workload(pkg, name):
+    if name == "rmat_lj":
+        return pkg.graphs.rmat_lj()
+    return pkg.graphs.rmat_s16()
+
+
+def config(name, g):
+    return {"workload": f"{name}: R-MAT a,b,c=.57/.19/.19, V={g.V}, E={g.E}"
+                        + (", ids permuted, seed 3" if name == "rmat_lj" else ", seed 1"),
+            "queries_per_step": {"bfs": N_BFS, "sssp": N_SSSP},
+            "sssp_weights": "GIR::edgeWeight hash in [1,100] (the reference's), delta 16",
+            "l2": "inputs larger than L2 (graph ~1.6 GB resident)",
+            "parallelism": "replicas (one full graph per GPU, queries split by rank)"}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch(kernel):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_sample(pkg, g, n_bfs, n_sssp, seed):
+    """The reference GIR (compiled from its sources) on this host's cores: bfs / sssp per source."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    kind = "reference" if oracle.ref_available() else "port"
+    src = pkg.graphs.sources_with_edges(g, max(n_bfs, n_sssp), seed)
+    outdeg = np.diff(g.fw_beg).astype(np.int64)
+    edges = 0
+    t_total = 0.0
+    if kind == "reference":
+        r = oracle.RefGIR(g.V, g.fw_beg, g.fw_adj, g.bw_beg, g.bw_adj)
+        r.bfs(int(src[0]))  # warm (page faults of the query arrays)
+        for s in src[:n_bfs]:
+            t = time.perf_counter(); lv = r.bfs(int(s)); t_total += time.perf_counter() - t
+            edges += int(outdeg[lv >= 0].sum())
+        for s in src[:n_sssp]:
+            t = time.perf_counter(); d = r.sssp(int(s), DELTA); t_total += time.perf_counter() - t
+            edges += int(outdeg[d != np.iinfo(np.uint64).max].sum())
+        r.close()
+    else:
+        fb = g.fw_beg.astype(np.int64)
+        for s in src[:n_bfs]:
+            t = time.perf_counter(); lv = oracle.bfs(g.V, fb, g.fw_adj, [s]); t_total += time.perf_counter() - t
+            edges += int(outdeg[lv >= 0].sum())
+        for s in src[:n_sssp]:
+            t = time.perf_counter(); d = oracle.sssp(g.V, fb, g.fw_adj, [s]); t_total += time.perf_counter() - t
+            edges += int(outdeg[d != np.iinfo(np.uint64).max].sum())
+    return edges, t_total, kind
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    pkg = importlib.import_module("graph-intermedia-representation_b200")
+    g = workload(pkg, args.workload)
+    n_bfs, n_sssp = 4, 1
+    for w in range(args.warmup):
+        cpu_reference_sample(pkg, g, 1, 0, 100 + w)
+    edges = 0
+    t = 0.0
+    kind = "reference"
+    for s in range(args.steps):
+        e, dt, kind = cpu_reference_sample(pkg, g, n_bfs, n_sssp, 7 + s)
+        edges += e
+        t += dt
+    gteps = edges / t / 1e9
+    cores = int(os.environ["OMP_NUM_THREADS"])
+    sample = f"{n_bfs} bfs + {n_sssp} sssp(delta={DELTA}) sources per step of the same graph"
+    line = {"impl": "reference", "metric": METRIC, "value": gteps, "unit": "GTEPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32 levels, uint64 sums",
+            "data": "synthetic", "config": config(args.workload, g),
+            "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    pkg = importlib.import_module("graph-intermedia-representation_b200")
+    native = pkg.native
+    g = workload(pkg, args.workload)
+    d = pkg.DeviceGraph.from_graph(g)
+    stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
+    V = g.V
+    src_bfs = pkg.graphs.sources_with_edges(g, N_BFS, 11 + 1000 * rank)
+    src_sssp = pkg.graphs.sources_with_edges(g, N_SSSP, 12 + 1000 * rank)
+    dev = f"cuda:{local}"
+    lv_d = torch.empty((N_BFS, V), dtype=torch.int32, device=dev)
+    ds_d = torch.empty((N_SSSP, V), dtype=torch.int64, device=dev)
+    sb_d = torch.from_numpy(src_bfs).to(dev)
+    ss_d = torch.from_numpy(src_sssp).to(dev)
+
+    def step(lv, ds, sb, ss):
+        d.bfs(sb, out=lv)
+        qb = d.query_stats()
+        d.sssp(ss, delta=DELTA, weights=native.WEIGHT_HASH, out=ds)
+        qs = d.query_stats()
+        return qb, qs
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+
+    def timed(fn, steps):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        ev0.record(stream)
+        stats = [fn() for _ in range(steps)]
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        if pg is not None:
+            t = torch.tensor([ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, stats
+
+    for _ in range(args.warmup):
+        step(lv_d, ds_d, sb_d, ss_d)
+    clocks = Clocks(local)
+    clocks.start()
+    ms, stats = timed(lambda: step(lv_d, ds_d, sb_d, ss_d), args.steps)
+    clk = clocks.stop()
+    edges_step = stats[0][0]["edges"] + stats[0][1]["edges"]
+    bfs_ms = sum(s[0]["total_ms"] for s in stats) / args.steps
+    sssp_ms = sum(s[1]["total_ms"] for s in stats) / args.steps
+    launches = sum(s[0]["launches"] + s[1]["launches"] for s in stats)
+    total_edges = edges_step * args.steps * world
+    value = total_edges / (ms * 1e-3) / 1e9
+
+    # e2e: pinned host buffers through the same C-ABI calls
+    lv_h = torch.empty((N_BFS, V), dtype=torch.int32, pin_memory=True)
+    ds_h = torch.empty((N_SSSP, V), dtype=torch.int64, pin_memory=True)
+    sb_h = torch.from_numpy(src_bfs).pin_memory()
+    ss_h = torch.from_numpy(src_sssp).pin_memory()
+    step(lv_h, ds_h, sb_h, ss_h)
+    ms_e2e, _ = timed(lambda: step(lv_h, ds_h, sb_h, ss_h), args.steps)
+    e2e = {"value": total_edges / (ms_e2e * 1e-3) / 1e9, "unit": "GTEPS",
+           "h2d_bytes_per_step": int(sb_h.numel() * 4 + ss_h.numel() * 4),
+           "d2h_bytes_per_step": int(lv_h.numel() * 4 + ds_h.numel() * 8), "ms_per_step": ms_e2e / args.steps}
+    # parity spot check of the e2e results against the device-resident run
+    assert torch.equal(lv_h, lv_d.cpu()) and torch.equal(ds_h, ds_d.cpu()), "host and device runs disagree"
+
+    # roofline of the dominant kernel (live CUDA events around its launches)
+    d.set_param(native.PARAM_PROFILE, 1)
+    qb, qs = step(lv_d, ds_d, sb_d, ss_d)
+    d.set_param(native.PARAM_PROFILE, 0)
+    bfs_bytes = 4 * qb["edges"] + 12 * qb["reached"] + 4 * V * N_BFS
+    sssp_bytes = 8 * qs["edges"] + 16 * qs["reached"] + 8 * V * N_SSSP
+    if qs["main_ms"] >= qb["main_ms"]:
+        kern, kb, kms, kl = "k_relax (SSSP)", sssp_bytes, qs["main_ms"], qs["main_launches"]
+    else:
+        kern, kb, kms, kl = "BFS level kernels", bfs_bytes, qb["main_ms"], qb["main_launches"]
+    peak, peak_src = measured_peak()
+    achieved = kb / (kms * 1e-3) / 1e9
+    tr = traffic_per_launch(kern)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": tr, "kernel": kern, "launches": kl, "kernel_ms": kms,
+                "algorithmic_bytes": kb, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"}
+
+    # SSSP with the stored U[1,255] weights (the configuration's weights), reported beside
+    d.sssp(ss_d, delta=DELTA, weights=native.WEIGHT_STORED, out=ds_d)
+    qst = d.query_stats()
+    extra = {"bfs_gteps": stats[0][0]["edges"] / (bfs_ms * 1e-3) / 1e9,
+             "sssp_gteps": stats[0][1]["edges"] / (sssp_ms * 1e-3) / 1e9,
+             "sssp_stored_u255_gteps": qst["edges"] / (qst["total_ms"] * 1e-3) / 1e9,
+             "bfs_ms_per_64": bfs_ms, "sssp_ms_per_64": sssp_ms}
+
+    # layer builds and update batches (every layer kept exact)
+    upd = {}
+    if not args.no_updates:
+        def ev_time(fn):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+        builds = {"wcc_ms": ev_time(lambda: d.build(native.LAYER_WCC)),
+                  "scc_dag_ms": ev_time(lambda: d.build(native.LAYER_SCC)),
+                  "bct_ms": ev_time(lambda: d.build(native.LAYER_BCT))}
+        extra["build"] = builds
+        for n in (10_000, 100_000, 1_000_000):
+            u, v, ins = pkg.graphs.updates(g, n // 2, n // 2, 50 + n + rank)
+            ub, vb, ib = (torch.from_numpy(x).pin_memory() for x in (u, v, ins))
+            t = ev_time(lambda: d.apply_batch(ub.numpy(), vb.numpy(), ib.numpy()))
+            upd[str(n)] = n / (t * 1e-3)
+        extra["updates_per_s"] = upd
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+        nb, ns = 16, 4
+        e, t, kind = cpu_reference_sample(pkg, g, nb, ns, 7)
+        cpu = {"value": e / t / 1e9, "unit": "GTEPS", "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())),
+               "kind": kind, "sample": f"{nb} bfs + {ns} sssp(delta={DELTA}) sources of the same graph "
+                                       f"(sources with out-edges), {t:.1f} s wall on the host cores"}
+    line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32 levels, uint64 distance sums", "data": "synthetic",
+            "config": config(args.workload, g), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clk, "gpu_launches": int(launches), **extra}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    d.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -316,6 +316,7 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
     const double alpha = g->params[GIR_PARAM_ALPHA], beta = g->params[GIR_PARAM_BETA];
     const int64_t E = g->fw.E;
     const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
+    MainTimer timer{g, g->params[GIR_PARAM_PROFILE] != 0.0};
     GIR_CUDA(g, cudaEventRecord(g->ev0, g->stream));
 
     for (int64_t g0 = 0; g0 < n_sets; g0 += 64) {
@@ -384,9 +385,12 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
                     const int64_t warps_per_block = kBlock / 32;
                     int64_t blocks = (chunks + warps_per_block - 1) / warps_per_block;
                     if (blocks > grid) blocks = grid;
-                    k_td_expand<<<(int)blocks, kBlock, 0, g->stream>>>(qa, nq, pref, total, view(g->fw), front, seen,
-                                                                       next, qb, cnt);
-                    GIR_LAUNCH(g, "k_td_expand");
+                    GIR_TRY(timer.run([&]() -> int {
+                        k_td_expand<<<(int)blocks, kBlock, 0, g->stream>>>(qa, nq, pref, total, view(g->fw), front,
+                                                                           seen, next, qb, cnt);
+                        GIR_LAUNCH(g, "k_td_expand");
+                        return GIR_OK;
+                    }));
                 }
                 k_clear_front<<<grid_for(g, nq, kBlock), kBlock, 0, g->stream>>>(qa, nq, front);
                 GIR_LAUNCH(g, "k_clear_front");
@@ -401,27 +405,30 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
                 st.launches += 4;
             } else {
                 const int32_t* bins = static_cast<const int32_t*>(g->bins.p);
-                if (g->bin_n[0] > 0) {
-                    k_bu_thread<<<grid_for(g, g->bin_n[0], kBlock), kBlock, 0, g->stream>>>(
-                        bins, g->bin_n[0], view(g->bw), front, seen, next, all, g->fw.deg, level, V, L + 1, qa, cnt);
-                    GIR_LAUNCH(g, "k_bu_thread");
-                    st.launches++;
-                }
-                if (g->bin_n[1] > 0) {
-                    k_bu_warp<<<grid_for(g, g->bin_n[1] * 32, kBlock), kBlock, 0, g->stream>>>(
-                        bins + g->bin_n[0], g->bin_n[1], view(g->bw), front, seen, next, all, g->fw.deg, level, V, L + 1,
-                        qa, cnt);
-                    GIR_LAUNCH(g, "k_bu_warp");
-                    st.launches++;
-                }
-                if (g->bin_n[2] > 0) {
-                    const int64_t b = g->bin_n[2] < grid ? g->bin_n[2] : grid;
-                    k_bu_cta<<<(int)b, kBlock, 0, g->stream>>>(bins + g->bin_n[0] + g->bin_n[1], g->bin_n[2],
-                                                               view(g->bw), front, seen, next, all, g->fw.deg, level, V,
-                                                               L + 1, qa, cnt);
-                    GIR_LAUNCH(g, "k_bu_cta");
-                    st.launches++;
-                }
+                GIR_TRY(timer.run([&]() -> int {
+                    if (g->bin_n[0] > 0) {
+                        k_bu_thread<<<grid_for(g, g->bin_n[0], kBlock), kBlock, 0, g->stream>>>(
+                            bins, g->bin_n[0], view(g->bw), front, seen, next, all, g->fw.deg, level, V, L + 1, qa, cnt);
+                        GIR_LAUNCH(g, "k_bu_thread");
+                        st.launches++;
+                    }
+                    if (g->bin_n[1] > 0) {
+                        k_bu_warp<<<grid_for(g, g->bin_n[1] * 32, kBlock), kBlock, 0, g->stream>>>(
+                            bins + g->bin_n[0], g->bin_n[1], view(g->bw), front, seen, next, all, g->fw.deg, level, V,
+                            L + 1, qa, cnt);
+                        GIR_LAUNCH(g, "k_bu_warp");
+                        st.launches++;
+                    }
+                    if (g->bin_n[2] > 0) {
+                        const int64_t b = g->bin_n[2] < grid ? g->bin_n[2] : grid;
+                        k_bu_cta<<<(int)b, kBlock, 0, g->stream>>>(bins + g->bin_n[0] + g->bin_n[1], g->bin_n[2],
+                                                                   view(g->bw), front, seen, next, all, g->fw.deg, level,
+                                                                   V, L + 1, qa, cnt);
+                        GIR_LAUNCH(g, "k_bu_cta");
+                        st.launches++;
+                    }
+                    return GIR_OK;
+                }));
                 std::swap(front, next);
                 next_dirty = true;
                 st.bottom_up++;

@@ -216,6 +216,8 @@ int create_impl(const int32_t* fw_beg, const int32_t* fw_adj, const int32_t* bw_
     GIR_CUDA(g, cudaEventCreate(&g->ev1));
     GIR_CUDA(g, cudaEventCreate(&g->ev2));
     GIR_CUDA(g, cudaEventCreate(&g->ev3));
+    GIR_CUDA(g, cudaEventCreate(&g->pev0));
+    GIR_CUDA(g, cudaEventCreate(&g->pev1));
     g->V = V;
     g->wrule_lo = 1;  // lo > hi: inserted edges get the hash weight of GIR::edgeWeight
     g->wrule_hi = 0;
@@ -511,8 +513,10 @@ int gir_dev_destroy(gir_dev_t* g) {
     for (auto& b : g->scratch) release(b);
     for (auto& b : g->work) release(b);
     release(g->cub_tmp); release(g->stage_in); release(g->stage_out); release(g->sched_w);
+    release(g->sched_io); release(g->lane_dist);
+    for (auto& b : g->qitems) release(b);
     if (g->pinned) cudaFreeHost(g->pinned);
-    for (cudaEvent_t e : {g->ev0, g->ev1, g->ev2, g->ev3}) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {g->ev0, g->ev1, g->ev2, g->ev3, g->pev0, g->pev1}) if (e) cudaEventDestroy(e);
     if (g->stream) cudaStreamDestroy(g->stream);
     delete g;
     return GIR_OK;
@@ -691,7 +695,7 @@ int gir_dev_set_schedule(gir_dev_t* g, int mode) {
 int gir_dev_set_param(gir_dev_t* g, int which, double value) {
     if (!g) return GIR_ERR_INVALID;
     if (which < 0 || which >= GIR_PARAM_COUNT) return fail(g, GIR_ERR_INVALID, "unknown parameter");
-    if (!(value > 0)) return fail(g, GIR_ERR_INVALID, "parameters are positive");
+    if (!(value > 0) && which != GIR_PARAM_PROFILE) return fail(g, GIR_ERR_INVALID, "parameters are positive");
     if (which == GIR_PARAM_BLOCK && ((int)value % 32 != 0 || value > 1024)) return fail(g, GIR_ERR_INVALID, "block: multiple of 32, <= 1024");
     g->params[which] = value;
     if (which == GIR_PARAM_SMALL_DEG || which == GIR_PARAM_LARGE_DEG) g->bins_valid = false;
@@ -714,6 +718,8 @@ int gir_dev_query_stats(gir_dev_t* g, gir_dev_query_stats_t* out) {
     out->launches = g->qstats.launches;
     out->kernel_ms = g->qstats.kernel_ms;
     out->total_ms = g->qstats.total_ms;
+    out->main_ms = g->qstats.main_ms;
+    out->main_launches = g->qstats.main_launches;
     return GIR_OK;
 }
 

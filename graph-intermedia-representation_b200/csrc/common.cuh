@@ -61,7 +61,17 @@ inline CSRView view(const DevCSR& c) { return CSRView{c.beg, c.deg, c.adj, c.w};
 
 struct QueryStats {
     int64_t edges = 0, reached = 0, iterations = 0, bottom_up = 0, launches = 0;
-    double kernel_ms = 0, total_ms = 0;
+    double kernel_ms = 0, total_ms = 0, main_ms = 0;
+    int64_t main_launches = 0;
+};
+
+// Times the launches issued by `launch` with CUDA events when profiling is on, adding them to
+// the query statistics (the caller synchronizes the stream before reading the result).
+struct MainTimer {
+    gir_dev* g;
+    bool on;
+    template <class F>
+    int run(F&& launch);
 };
 
 }  // namespace gir
@@ -102,6 +112,8 @@ struct gir_dev {
     gir::DevBuf cub_tmp;
     gir::DevBuf stage_in, stage_out;  // device staging for host pointers
     gir::DevBuf work[8];              // buffers of the create / batch pipelines (not used by store ops)
+    gir::DevBuf lane_dist;            // lane-interleaved SSSP distances (V x lanes)
+    gir::DevBuf qitems[5];            // per-queue-entry work items of the SSSP relaxation
     void* pinned = nullptr;           // small pinned host buffer for counters
     size_t pinned_bytes = 0;
 
@@ -110,7 +122,8 @@ struct gir_dev {
 
     // Schedule
     int schedule = GIR_SCHEDULE_FIXED;
-    double params[GIR_PARAM_COUNT] = {15.0, 18.0, 16.0, 256.0, 32.0, 4096.0, 4.0};
+    double params[GIR_PARAM_COUNT] = {15.0, 18.0, 16.0, 256.0, 32.0, 4096.0, 4.0, 0.0};
+    cudaEvent_t pev0 = nullptr, pev1 = nullptr;  // main-kernel timing (GIR_PARAM_PROFILE)
     gir::DevBuf sched_w;              // MLP parameters (fp32)
     gir::DevBuf sched_io;             // one decision's features and logits
     bool sched_loaded = false;
@@ -153,6 +166,20 @@ inline int grid_for(gir_dev* g, int64_t work, int block) {
     const int64_t blocks = (work + block - 1) / block;
     const int64_t cap = (int64_t)g->num_sms * (int64_t)g->params[GIR_PARAM_CTAS_PER_SM] * 4;
     return (int)(blocks < 1 ? 1 : (blocks < cap ? blocks : cap));
+}
+
+template <class F>
+int MainTimer::run(F&& launch) {
+    if (!on) return launch();
+    GIR_CUDA(g, cudaEventRecord(g->pev0, g->stream));
+    GIR_TRY(launch());
+    GIR_CUDA(g, cudaEventRecord(g->pev1, g->stream));
+    GIR_CUDA(g, cudaEventSynchronize(g->pev1));
+    float ms = 0;
+    GIR_CUDA(g, cudaEventElapsedTime(&ms, g->pev0, g->pev1));
+    g->qstats.main_ms += ms;
+    g->qstats.main_launches++;
+    return GIR_OK;
 }
 
 // ---- store (store.cu) ----

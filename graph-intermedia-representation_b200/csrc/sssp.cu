@@ -1,17 +1,20 @@
-// Delta-stepping single-source shortest paths on the device (GIR::sssp / deltaStepping,
-// gir_query.cpp:629-703): uint64 distances, UINT64_MAX = unreachable.
+// Delta-stepping shortest paths on the device (GIR::sssp / deltaStepping, gir_query.cpp:629-703):
+// uint64 distances, UINT64_MAX = unreachable.
 //
-// Buckets of width Delta are processed in increasing order. Within bucket k the near queue is
-// relaxed through its light edges (weight < Delta) round after round until no vertex re-enters
-// the bucket; then every vertex settled in the bucket relaxes its heavy edges (weight >= Delta)
-// once -- those can only land in later buckets. (The reference relaxes all edges every round and
-// has no light/heavy split, gir_query.cpp:674-688; the split changes the work, not the result.)
-// Relaxations that land beyond the bucket go to a far queue, which is split by the next
-// non-empty bucket (dist / Delta of its smallest live entry).
-//
-// Rows are read from a weight-sorted copy of the forward CSR, so the light edges of a row are a
-// prefix of it and the heavy edges the rest. Shortest distances are unique, so the result is
-// the same for every Delta and every schedule.
+// Up to 64 queries run as one traversal (lanes), like the BFS: every vertex carries 64-bit lane
+// masks for the work of the current bucket (near), for relaxations beyond it (far) and for the
+// lanes settled in the bucket; distances are stored lane-interleaved (dist[v * lanes + s]) so a
+// warp relaxing one edge for many lanes touches one contiguous row. All lanes step through the
+// buckets together, each lane running exact Delta-stepping:
+//  - bucket k = [k*Delta, (k+1)*Delta): the near vertices relax their light edges
+//    (weight < Delta) round after round until no lane re-enters the bucket;
+//  - then every (vertex, lane) settled in the bucket relaxes its heavy edges (weight >= Delta)
+//    once -- those land in later buckets only. (The reference relaxes all edges every round and
+//    has no light/heavy split, gir_query.cpp:674-688; the split changes the work, not the result.)
+//  - the next bucket is the smallest live far distance; the far entries inside it become near.
+// Rows are read from a weight-sorted copy of the forward CSR, so a row's light edges are its
+// prefix. Shortest distances are unique, so the result is the same for every Delta, every
+// schedule and every lane grouping.
 #include "common.cuh"
 
 namespace gir {
@@ -20,14 +23,15 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kWarps = kBlock / 32;
+constexpr uint64_t kInf = ~0ull;
 
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-// counters: [0] near queue length being built, [1] far queue length, [2] settled list length,
-// [3] min far distance (atomicMin), [4] far queue length after a split, [8] length of the queue
-// being relaxed; accumulated over the queries: [16] reached vertices, [17] their out-edges
-enum { S_NEAR = 0, S_FAR = 1, S_SET = 2, S_MIN = 3, S_FAR2 = 4, S_QLEN = 8, S_REACHED = 16, S_EDGES = 17, S_N = 8 };
+// counters: [0] next near queue length, [1] far queue length, [2] settled queue length,
+// [3] min live far distance, [4] far queue length after a split, [8] length of the queue being
+// read; accumulated over the call: [16] reached (vertex, lane) pairs, [17] their out-edges
+enum { S_NEAR = 0, S_FAR = 1, S_SET = 2, S_MIN = 3, S_FAR2 = 4, S_QLEN = 8, S_REACHED = 16, S_EDGES = 17, S_N = 32 };
 
 __global__ void k_ws_keys(int64_t V, int64_t E, const int64_t* cb, CSRView c, int hash, uint64_t* keys,
                           uint32_t* cols) {
@@ -58,141 +62,194 @@ __global__ void k_deg_i64(int64_t V, const int32_t* deg, int64_t* out) {
     if (blockIdx.x == 0 && threadIdx.x == 0) out[V] = 0;
 }
 
-__global__ void k_sssp_init(const int32_t* srcs, int64_t n, int64_t V, uint64_t* dist, int32_t* near_mark,
-                            int32_t epoch, int32_t* nearq, unsigned long long* cnt) {
-    GRID_STRIDE(i, n) {
-        const int32_t s = srcs[i];
-        if (s < 0 || s >= V) continue;
-        dist[s] = 0;
-        if (atomicExch(&near_mark[s], epoch) != epoch) nearq[atomicAdd(&cnt[S_NEAR], 1ull)] = s;
+// Lane s of the group starts at every vertex of set s (set_beg: device copy, absolute offsets).
+__global__ void k_sssp_init(const int64_t* set_beg, int nl, const int32_t* srcs, int64_t V, uint64_t* dist,
+                            unsigned long long* nearmask, int32_t* nearq, unsigned long long* cnt) {
+    const int64_t lo = set_beg[0], hi = set_beg[nl];
+    GRID_STRIDE(i, hi - lo) {
+        const int64_t e = lo + i;
+        int s = 0;
+        while (set_beg[s + 1] <= e) ++s;
+        const int32_t v = srcs[e];
+        if (v < 0 || v >= V) continue;
+        dist[(int64_t)v * nl + s] = 0;
+        if (atomicOr(&nearmask[v], 1ull << s) == 0ull) nearq[atomicAdd(&cnt[S_NEAR], 1ull)] = v;
     }
 }
 
-struct RelaxArgs {
-    const int64_t* wb;      // weight-sorted rows (compact offsets)
+// Index of the k-th set bit of a 64-bit mask (k < popcount).
+__device__ __forceinline__ int nth_bit(uint64_t m, int k) {
+    const unsigned lo = (unsigned)m;
+    const int cl = __popc(lo);
+    if (k < cl) return __fns(lo, 0, k + 1);
+    return 32 + __fns((unsigned)(m >> 32), 0, k - cl + 1);
+}
+
+struct Relax {
+    const int64_t* wb;       // weight-sorted rows (compact offsets)
     const int32_t* wdeg;
     const int32_t* wadj;
     const uint32_t* ww;
-    uint64_t delta, kend;   // bucket width; end of the current bucket
+    uint64_t delta, kend;    // bucket width; end of the current bucket
+    int nl;                  // lanes (row stride of dist)
     uint64_t* dist;
-    int32_t* near_mark; int32_t near_epoch; int32_t* nearq;
-    int32_t* far_mark; int32_t far_epoch; int32_t* farq;
-    int32_t* settle_mark; int32_t settle_epoch; int32_t* setq;
+    unsigned long long* curmask;   // lanes of each queued vertex to process (read and cleared)
+    unsigned long long* nextmask;  // lanes re-entering the bucket
+    int32_t* nextq;
+    unsigned long long* farmask;
+    int32_t* farq;
+    unsigned long long* setmask;   // lanes settled in this bucket
+    int32_t* setq;
     unsigned long long* cnt;
 };
 
-// Relaxes the light (heavy = 0) or heavy (heavy = 1) edges of the queue's vertices. A warp takes
-// 32 queue entries at a time and walks their edge ranges together: lane l handles positions
-// l, l+32, ... of the concatenated ranges (owner found by binary search in shared memory).
-__global__ void __launch_bounds__(kBlock) k_relax(const int32_t* q, const unsigned long long* qlen, int heavy,
-                                                  RelaxArgs a) {
-    __shared__ int64_t s_excl[kWarps][33];
-    __shared__ int64_t s_eb[kWarps][32];
-    __shared__ uint64_t s_du[kWarps][32];
-    __shared__ int32_t s_u[kWarps][32];
-    const int lane = lane_id(), wib = threadIdx.x >> 5;
-    const int64_t n = (int64_t)*qlen;
+// Work-balanced relaxation, in two kernels. k_relax_prep takes every queued vertex's lanes (and
+// clears them), does the settle bookkeeping and stores the vertex's edge range and lane mask with
+// its work (edges x lanes); after an exclusive scan of the work, k_relax_run cuts the whole
+// queue's (edge, lane) pairs into equal chunks, so a hub with many lanes is spread over the grid
+// instead of one warp. Pairs are enumerated edge-major within a vertex: with many lanes active,
+// consecutive threads update consecutive lanes of one distance row.
+struct Items {
+    int32_t* u;
+    int64_t* eb;
+    unsigned long long* m;
+    int32_t* pc;
+    int64_t* pref;  // work per entry, then its exclusive scan (n + 1 entries)
+};
+
+__global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, Items it) {
+    GRID_STRIDE(i, n) {
+        const int32_t u = q[i];
+        unsigned long long m;
+        if (heavy) {
+            m = a.setmask[u];
+            a.setmask[u] = 0ull;
+        } else {
+            m = a.curmask[u];
+            a.curmask[u] = 0ull;
+            if (m && atomicOr(&a.setmask[u], m) == 0ull) a.setq[atomicAdd(&a.cnt[S_SET], 1ull)] = u;
+        }
+        const int pc = __popcll(m);
+        const int64_t b = a.wb[u], e = b + a.wdeg[u];
+        int64_t lo = b, hi = e;  // light edges: the prefix with weight < delta
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if ((uint64_t)a.ww[mid] < a.delta) lo = mid + 1; else hi = mid;
+        }
+        it.u[i] = u;
+        it.eb[i] = heavy ? lo : b;
+        it.m[i] = m;
+        it.pc[i] = pc;
+        it.pref[i] = (heavy ? e - lo : lo - b) * pc;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) it.pref[n] = 0;
+}
+
+constexpr int kChunk = 32 * 8;  // (edge, lane) pairs per warp chunk
+
+__global__ void __launch_bounds__(kBlock) k_relax_run(int64_t n, Items it, Relax a) {
+    const int64_t total = it.pref[n];  // (after the scan: all pairs of the queue)
+    const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
-        const int64_t i = base + lane;
-        int64_t eb = 0, ecount = 0;
-        uint64_t du = 0;
-        int32_t u = -1;
-        if (i < n) {
-            u = q[i];
-            du = a.dist[u];
-            const int64_t b = a.wb[u], e = b + a.wdeg[u];
-            int64_t lo = b, hi = e;  // light edges: the prefix with weight < delta
-            while (lo < hi) {
-                const int64_t m = (lo + hi) >> 1;
-                if ((uint64_t)a.ww[m] < a.delta) lo = m + 1; else hi = m;
-            }
-            if (heavy) { eb = lo; ecount = e - lo; }
-            else { eb = b; ecount = lo - b; }
-            if (!heavy && atomicExch(&a.settle_mark[u], a.settle_epoch) != a.settle_epoch)
-                a.setq[atomicAdd(&a.cnt[S_SET], 1ull)] = u;
+    for (int64_t c0 = warp * kChunk; c0 < total; c0 += nwarps * kChunk) {
+        const int64_t c1 = c0 + kChunk < total ? c0 + kChunk : total;
+        const int64_t key = c0 + lane < total ? c0 + lane : total - 1;
+        int64_t lo = 0, hi = n - 1;  // entry owning this lane's first pair
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) >> 1;
+            if (it.pref[mid] <= key) lo = mid; else hi = mid - 1;
         }
-        int64_t incl = ecount;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        s_excl[wib][lane] = incl - ecount;
-        if (lane == 31) s_excl[wib][32] = incl;
-        s_eb[wib][lane] = eb;
-        s_du[wib][lane] = du;
-        s_u[wib][lane] = u;
-        __syncwarp();
-        const int64_t total = s_excl[wib][32];
-        for (int64_t p0 = 0; p0 < total; p0 += 32) {
-            const int64_t p = p0 + lane;
+        int64_t i = lo;
+        for (int64_t base = c0; base < c1; base += 32) {  // warp-uniform
+            const int64_t p = base + lane;
             bool to_near = false, to_far = false;
             int32_t w = 0;
-            if (p < total) {
-                int lo = 0, hi = 31;  // largest l with excl[l] <= p
-                while (lo < hi) {
-                    const int m = (lo + hi + 1) >> 1;
-                    if (s_excl[wib][m] <= p) lo = m; else hi = m - 1;
-                }
-                const int64_t k = s_eb[wib][lo] + (p - s_excl[wib][lo]);
+            if (p < c1) {
+                while (it.pref[i + 1] <= p) ++i;
+                const int32_t q2 = (int32_t)(p - it.pref[i]);
+                const int pcl = it.pc[i];
+                const int64_t k = it.eb[i] + q2 / pcl;
+                const int s = nth_bit(it.m[i], q2 % pcl);
+                const int32_t uu = it.u[i];
                 w = a.wadj[k];
-                const uint64_t nd = s_du[wib][lo] + (uint64_t)a.ww[k];
-                const unsigned long long old = atomicMin((unsigned long long*)&a.dist[w], (unsigned long long)nd);
-                if (nd < old) {
-                    if (nd < a.kend) to_near = atomicExch(&a.near_mark[w], a.near_epoch) != a.near_epoch;
-                    else to_far = atomicExch(&a.far_mark[w], a.far_epoch) != a.far_epoch;
+                const uint64_t nd = a.dist[(int64_t)uu * a.nl + s] + (uint64_t)a.ww[k];
+                uint64_t* dw = &a.dist[(int64_t)w * a.nl + s];
+                if (nd < *(volatile uint64_t*)dw) {  // plain pre-check: most relaxations lose
+                    const unsigned long long old = atomicMin((unsigned long long*)dw, (unsigned long long)nd);
+                    if (nd < old) {
+                        const unsigned long long bit = 1ull << s;
+                        if (nd < a.kend) to_near = atomicOr(&a.nextmask[w], bit) == 0ull;
+                        else to_far = atomicOr(&a.farmask[w], bit) == 0ull;
+                    }
                 }
             }
-            warp_append(to_near, w, a.nearq, &a.cnt[S_NEAR]);
+            warp_append(to_near, w, a.nextq, &a.cnt[S_NEAR]);
             warp_append(to_far, w, a.farq, &a.cnt[S_FAR]);
         }
-        __syncwarp();
     }
 }
 
-// Smallest distance among live far entries (dist >= kend; smaller ones are settled already).
-__global__ void k_far_min(const int32_t* farq, const unsigned long long* nfar, const uint64_t* dist, uint64_t kend,
-                          unsigned long long* cnt) {
-    unsigned long long m = ~0ull;
+// Smallest live far distance (dist >= kend; smaller ones are settled already).
+__global__ void k_far_min(const int32_t* farq, const unsigned long long* nfar, const unsigned long long* farmask,
+                          const uint64_t* dist, int nl, uint64_t kend, unsigned long long* cnt) {
+    unsigned long long mn = kInf;
     const int64_t n = (int64_t)*nfar;
     GRID_STRIDE(i, n) {
-        const uint64_t d = dist[farq[i]];
-        if (d >= kend && d < m) m = d;
+        const int32_t w = farq[i];
+        unsigned long long m = farmask[w];
+        while (m) {
+            const int s = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            const uint64_t d = dist[(int64_t)w * nl + s];
+            if (d >= kend && d < mn) mn = d;
+        }
     }
     for (int o = 16; o; o >>= 1) {
-        const unsigned long long t = __shfl_xor_sync(0xffffffffu, m, o);
-        m = t < m ? t : m;
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, mn, o);
+        mn = t < mn ? t : mn;
     }
-    if (lane_id() == 0 && m != ~0ull) atomicMin(&cnt[S_MIN], m);
+    if (lane_id() == 0 && mn != kInf) atomicMin(&cnt[S_MIN], mn);
 }
 
-// Splits the far queue at the new bucket [lo, hi): entries in it go to the near queue, later
-// ones to farq2, settled (stale) ones are dropped; duplicates are dropped by the marks.
-__global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar, const uint64_t* dist, uint64_t lo,
-                            uint64_t hi, int32_t* near_mark, int32_t near_epoch, int32_t* nearq, int32_t* far_mark,
-                            int32_t far_epoch, int32_t* farq2, unsigned long long* cnt) {
+// Splits the far entries at the new bucket [lo, hi): lanes inside it become near work, later
+// lanes stay far (queued in farq2), settled lanes are dropped.
+__global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar, unsigned long long* farmask,
+                            const uint64_t* dist, int nl, uint64_t lo, uint64_t hi, unsigned long long* nearmask,
+                            int32_t* nearq, int32_t* farq2, unsigned long long* cnt) {
     const int64_t n = (int64_t)*nfar;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
         bool to_near = false, to_far = false;
-        int32_t v = 0;
+        int32_t w = 0;
         if (i < n) {
-            v = farq[i];
-            const uint64_t d = dist[v];
-            if (d >= lo && d < hi) to_near = atomicExch(&near_mark[v], near_epoch) != near_epoch;
-            else if (d >= hi) to_far = atomicExch(&far_mark[v], far_epoch) != far_epoch;
+            w = farq[i];
+            unsigned long long m = farmask[w], nm = 0, keep = 0;
+            while (m) {
+                const int s = __ffsll((long long)m) - 1;
+                m &= m - 1;
+                const uint64_t d = dist[(int64_t)w * nl + s];
+                if (d >= lo && d < hi) nm |= 1ull << s;
+                else if (d >= hi) keep |= 1ull << s;
+            }
+            farmask[w] = keep;
+            to_far = keep != 0;
+            if (nm) to_near = atomicOr(&nearmask[w], nm) == 0ull;
         }
-        warp_append(to_near, v, nearq, &cnt[S_NEAR]);
-        warp_append(to_far, v, farq2, &cnt[S_FAR2]);
+        warp_append(to_near, w, nearq, &cnt[S_NEAR]);
+        warp_append(to_far, w, farq2, &cnt[S_FAR2]);
     }
 }
 
-// Reached vertices and their out-degrees (the traversed edges of the GTEPS figure).
-__global__ void k_sssp_reached(const uint64_t* dist, int64_t V, const int32_t* outdeg, unsigned long long* cnt) {
+// Reached (vertex, lane) pairs and their out-degrees (the traversed edges of the GTEPS figure).
+__global__ void k_sssp_reached(const uint64_t* dist, int64_t V, int nl, const int32_t* outdeg,
+                               unsigned long long* cnt) {
     unsigned long long r = 0, e = 0;
     GRID_STRIDE(v, V) {
-        if (dist[v] != ~0ull) { ++r; e += (unsigned long long)outdeg[v]; }
+        unsigned c = 0;
+        for (int s = 0; s < nl; ++s) c += dist[v * nl + s] != kInf;
+        r += c;
+        e += (unsigned long long)c * (unsigned long long)outdeg[v];
     }
     for (int o = 16; o; o >>= 1) {
         r += __shfl_xor_sync(0xffffffffu, r, o);
@@ -204,13 +261,31 @@ __global__ void k_sssp_reached(const uint64_t* dist, int64_t V, const int32_t* o
     }
 }
 
+// dist[v * nl + s] -> out[s * V + v], through 32 x 32 shared-memory tiles.
+__global__ void k_transpose(const uint64_t* dist, int64_t V, int nl, uint64_t* out) {
+    __shared__ uint64_t tile[32][33];
+    const int64_t v0 = (int64_t)blockIdx.x * 32;
+    const int s0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t v = v0 + r;
+        const int s = s0 + tx;
+        if (v < V && s < nl) tile[r][tx] = dist[v * nl + s];
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int s = s0 + r;
+        const int64_t v = v0 + tx;
+        if (v < V && s < nl) out[(int64_t)s * V + v] = tile[tx][r];
+    }
+}
+
 }  // namespace
 
 // Weight-sorted copy of the forward CSR for one weight mode (compact rows).
 static int build_weight_sorted(gir_dev* g, int hash, DevCSR& ws) {
     const int64_t V = g->V, E = g->fw.E;
     store_free(ws);
-    int64_t* cb = nullptr;
     uint64_t *keys = nullptr, *ktmp = nullptr;
     uint32_t *cols = nullptr, *ctmp = nullptr;
     GIR_CUDA(g, cudaMalloc(&ws.beg, sizeof(int64_t) * (V + 1)));
@@ -218,7 +293,7 @@ static int build_weight_sorted(gir_dev* g, int hash, DevCSR& ws) {
     GIR_CUDA(g, cudaMalloc(&ws.adj, sizeof(int32_t) * (E > 0 ? E : 1)));
     GIR_CUDA(g, cudaMalloc(&ws.w, sizeof(uint32_t) * (E > 0 ? E : 1)));
     ws.cap = ws.E = E;
-    cb = ws.beg;
+    int64_t* cb = ws.beg;
     k_deg_i64<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, g->fw.deg, cb);
     GIR_LAUNCH(g, "k_deg_i64");
     GIR_TRY(exclusive_scan_i64(g, cb, cb, V + 1));
@@ -251,129 +326,147 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         GIR_TRY(build_weight_sorted(g, hash, ws));
         g->ws_valid[hash ? 0 : 1] = true;
     }
-    int32_t *nearq = nullptr, *nearq2 = nullptr, *farq = nullptr, *farq2 = nullptr, *setq = nullptr;
-    int32_t *near_mark = nullptr, *far_mark = nullptr, *settle_mark = nullptr;
+    const int64_t nl_max = n_sets < 64 ? n_sets : 64;
+    int32_t *nearq = nullptr, *nextq = nullptr, *farq = nullptr, *farq2 = nullptr, *setq = nullptr;
+    unsigned long long *curmask = nullptr, *nextmask = nullptr, *farmask = nullptr, *setmask = nullptr;
     unsigned long long* cnt = nullptr;
+    int64_t* sbeg = nullptr;
+    uint64_t* idist = nullptr;
     GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &nearq));
-    GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &nearq2));
-    GIR_TRY(ensure_n(g, g->scratch[2], 2 * V + 2, &farq));
-    GIR_TRY(ensure_n(g, g->scratch[3], 2 * V + 2, &farq2));
+    GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &nextq));
+    GIR_TRY(ensure_n(g, g->scratch[2], V + 1, &farq));
+    GIR_TRY(ensure_n(g, g->scratch[3], V + 1, &farq2));
     GIR_TRY(ensure_n(g, g->scratch[4], V + 1, &setq));
-    GIR_TRY(ensure_n(g, g->scratch[5], V + 1, &near_mark));
-    GIR_TRY(ensure_n(g, g->scratch[6], V + 1, &far_mark));
-    GIR_TRY(ensure_n(g, g->scratch[7], V + 1, &settle_mark));
-    GIR_TRY(ensure_n(g, g->scratch[12], 32, &cnt));
+    GIR_TRY(ensure_n(g, g->scratch[5], V + 1, &curmask));
+    GIR_TRY(ensure_n(g, g->scratch[6], V + 1, &nextmask));
+    GIR_TRY(ensure_n(g, g->scratch[7], V + 1, &farmask));
+    GIR_TRY(ensure_n(g, g->scratch[12], V + 1, &setmask));
+    GIR_TRY(ensure_n(g, g->scratch[13], S_N, &cnt));
+    GIR_TRY(ensure_n(g, g->scratch[14], 65, &sbeg));
+    if (nl_max > 1) GIR_TRY(ensure_n(g, g->lane_dist, (size_t)V * nl_max + 1, &idist));
     unsigned long long* hc = nullptr;
     {
         void* h = nullptr;
         GIR_TRY(pinned(g, 256, &h));
         hc = static_cast<unsigned long long*>(h);
     }
+    auto read = [&]() -> int {
+        GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
+        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+        return GIR_OK;
+    };
     const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
+    MainTimer timer{g, g->params[GIR_PARAM_PROFILE] != 0.0};
+    Items items;
+    GIR_TRY(ensure_n(g, g->qitems[0], V + 1, &items.u));
+    GIR_TRY(ensure_n(g, g->qitems[1], V + 1, &items.eb));
+    GIR_TRY(ensure_n(g, g->qitems[2], V + 1, &items.m));
+    GIR_TRY(ensure_n(g, g->qitems[3], V + 1, &items.pc));
+    GIR_TRY(ensure_n(g, g->qitems[4], V + 2, &items.pref));
     GIR_CUDA(g, cudaEventRecord(g->ev0, g->stream));
-    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 32, g->stream));
-    for (int64_t s = 0; s < n_sets; ++s) {
-        uint64_t* dist = dist_d + s * V;
+    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * S_N, g->stream));
+    for (int64_t g0 = 0; g0 < n_sets; g0 += 64) {
+        const int nl = (int)((n_sets - g0) < 64 ? (n_sets - g0) : 64);
+        // (a group that ends on settled-only far entries leaves their lane bits behind)
+        GIR_CUDA(g, cudaMemsetAsync(curmask, 0, sizeof(unsigned long long) * V, g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(nextmask, 0, sizeof(unsigned long long) * V, g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(farmask, 0, sizeof(unsigned long long) * V, g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(setmask, 0, sizeof(unsigned long long) * V, g->stream));
+        uint64_t* dist = nl > 1 ? idist : dist_d + g0 * V;
+        if (nl > 1) GIR_CUDA(g, cudaMemsetAsync(dist, 0xff, sizeof(uint64_t) * V * nl, g->stream));
         uint64_t D = delta;
         if (D == 0) {
             if (g->schedule == GIR_SCHEDULE_LEARNED && g->sched_loaded) {
                 const double E = (double)g->fw.E;
                 float feat[GIR_SCHED_IN] = {(float)(E / V / 64.0), hash ? 0.5f : 1.f, (float)(g->num_sms / 148.0),
-                                            0.f, 0.f, 0.f, 0.f, 1.f};
+                                            (float)(nl / 64.0), 0.f, 0.f, 0.f, 1.f};
                 GIR_TRY(sched_choose_delta(g, feat, &D));
             } else {
                 D = (uint64_t)g->params[GIR_PARAM_DELTA];
             }
             if (D == 0) D = 16;
         }
-        GIR_CUDA(g, cudaMemsetAsync(near_mark, 0, sizeof(int32_t) * V, g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(far_mark, 0, sizeof(int32_t) * V, g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(settle_mark, 0, sizeof(int32_t) * V, g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * S_N, g->stream));
-        int32_t near_epoch = 1, far_epoch = 1, settle_epoch = 1;
-        const int64_t n_src = set_beg_h[s + 1] - set_beg_h[s];
-        if (n_src > 0) {
-            k_sssp_init<<<grid_for(g, n_src, kBlock), kBlock, 0, g->stream>>>(srcs_d + set_beg_h[s], n_src, V, dist,
-                                                                             near_mark, near_epoch, nearq, cnt);
+        GIR_CUDA(g, cudaMemcpyAsync(sbeg, set_beg_h + g0, sizeof(int64_t) * (nl + 1), cudaMemcpyHostToDevice, g->stream));
+        for (int k = 0; k < S_N; ++k)
+            if (k != S_REACHED && k != S_EDGES) hc[k] = 0;
+        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, g->stream));
+        const int64_t n_entries = set_beg_h[g0 + nl] - set_beg_h[g0];
+        if (n_entries > 0) {
+            k_sssp_init<<<grid_for(g, n_entries, kBlock), kBlock, 0, g->stream>>>(sbeg, nl, srcs_d, V, dist, curmask,
+                                                                                 nearq, cnt);
             GIR_LAUNCH(g, "k_sssp_init");
         }
-        unsigned long long* qlen = cnt + S_QLEN;
-        GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
-        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-        uint64_t k = 0;
+        GIR_TRY(read());
         int64_t n_near = (int64_t)hc[S_NEAR], n_far = 0;
-        RelaxArgs a;
-        a.wb = ws.beg; a.wdeg = ws.deg; a.wadj = ws.adj; a.ww = ws.w; a.delta = D; a.dist = dist;
-        a.near_mark = near_mark; a.far_mark = far_mark; a.settle_mark = settle_mark; a.setq = setq; a.cnt = cnt;
+        Relax a;
+        a.wb = ws.beg; a.wdeg = ws.deg; a.wadj = ws.adj; a.ww = ws.w; a.delta = D; a.nl = nl; a.dist = dist;
+        a.farmask = farmask; a.setmask = setmask; a.setq = setq; a.cnt = cnt;
+        uint64_t k = 0;
+        // one relaxation pass over queue q (n entries): prep, scan of the work, balanced run
+        auto relax = [&](const int32_t* q, int64_t n, int heavy) -> int {
+            k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, items);
+            GIR_LAUNCH(g, "k_relax_prep");
+            GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));
+            GIR_TRY(timer.run([&]() -> int {
+                k_relax_run<<<grid, kBlock, 0, g->stream>>>(n, items, a);
+                GIR_LAUNCH(g, "k_relax_run");
+                return GIR_OK;
+            }));
+            st.launches += 4;  // prep, the scan's two kernels, run
+            return GIR_OK;
+        };
         while (true) {
-            // ---- bucket k ----
             a.kend = (k + 1) * D;
-            a.settle_epoch = ++settle_epoch;
             GIR_CUDA(g, cudaMemsetAsync(cnt + S_SET, 0, sizeof(unsigned long long), g->stream));
+            // light rounds: nearq (lanes in curmask) -> nextq (lanes in nextmask)
             while (n_near > 0) {
-                // near queue (length cnt[S_NEAR]) -> move its length to qlen, reset the counter
-                GIR_CUDA(g, cudaMemcpyAsync(qlen, cnt + S_NEAR, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
-                                            g->stream));
                 GIR_CUDA(g, cudaMemsetAsync(cnt + S_NEAR, 0, sizeof(unsigned long long), g->stream));
-                a.near_epoch = ++near_epoch;
-                a.nearq = nearq2;
-                a.far_epoch = far_epoch;
-                a.farq = farq;
-                const int64_t blocks = (n_near + 31) / 32 / kWarps + 1;
-                k_relax<<<(int)(blocks < grid ? blocks : grid), kBlock, 0, g->stream>>>(nearq, qlen, 0, a);
-                GIR_LAUNCH(g, "k_relax(light)");
-                st.launches++;
+                a.curmask = curmask; a.nextmask = nextmask; a.nextq = nextq; a.farq = farq;
+                GIR_TRY(relax(nearq, n_near, 0));
                 st.iterations++;
-                std::swap(nearq, nearq2);
-                GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
-                GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+                std::swap(nearq, nextq);
+                std::swap(curmask, nextmask);
+                GIR_TRY(read());
                 n_near = (int64_t)hc[S_NEAR];
             }
-            // heavy edges of everything settled in this bucket
+            // heavy edges of the (vertex, lane) pairs settled in this bucket
             const int64_t n_set = (int64_t)hc[S_SET];
             if (n_set > 0) {
-                GIR_CUDA(g, cudaMemcpyAsync(qlen, cnt + S_SET, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
-                                            g->stream));
-                a.near_epoch = ++near_epoch;
-                a.nearq = nearq2;  // (heavy relaxations never land in this bucket)
-                a.farq = farq;
-                const int64_t blocks = (n_set + 31) / 32 / kWarps + 1;
-                k_relax<<<(int)(blocks < grid ? blocks : grid), kBlock, 0, g->stream>>>(setq, qlen, 1, a);
-                GIR_LAUNCH(g, "k_relax(heavy)");
-                st.launches++;
+                a.curmask = curmask; a.nextmask = nextmask; a.nextq = nextq; a.farq = farq;
+                GIR_TRY(relax(setq, n_set, 1));
             }
-            // next non-empty bucket from the far queue
+            // next bucket: the smallest live far distance
             GIR_CUDA(g, cudaMemsetAsync(cnt + S_MIN, 0xff, sizeof(unsigned long long), g->stream));
-            GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
-            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+            GIR_TRY(read());
             n_far = (int64_t)hc[S_FAR];
             if (n_far == 0) break;
-            k_far_min<<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(farq, cnt + S_FAR, dist, a.kend, cnt);
+            k_far_min<<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(farq, cnt + S_FAR, farmask, dist, nl, a.kend,
+                                                                            cnt);
             GIR_LAUNCH(g, "k_far_min");
-            GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
-            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+            GIR_TRY(read());
             const uint64_t mind = hc[S_MIN];
-            if (mind == ~0ull) break;  // only settled entries left
+            if (mind == kInf) break;  // only settled entries left
             k = mind / D;
             GIR_CUDA(g, cudaMemsetAsync(cnt + S_FAR2, 0, sizeof(unsigned long long), g->stream));
-            a.near_epoch = ++near_epoch;
-            ++far_epoch;
-            k_far_split<<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(farq, cnt + S_FAR, dist, k * D, (k + 1) * D,
-                                                                              near_mark, near_epoch, nearq, far_mark,
-                                                                              far_epoch, farq2, cnt);
+            k_far_split<<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(farq, cnt + S_FAR, farmask, dist, nl, k * D,
+                                                                              (k + 1) * D, curmask, nearq, farq2, cnt);
             GIR_LAUNCH(g, "k_far_split");
-            st.launches += 3;
+            st.launches += 2;
             std::swap(farq, farq2);
             GIR_CUDA(g, cudaMemcpyAsync(cnt + S_FAR, cnt + S_FAR2, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
                                         g->stream));
-            GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
-            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+            GIR_TRY(read());
             n_near = (int64_t)hc[S_NEAR];
         }
-        k_sssp_reached<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(dist, V, g->fw.deg, cnt);
+        k_sssp_reached<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(dist, V, nl, g->fw.deg, cnt);
         GIR_LAUNCH(g, "k_sssp_reached");
+        if (nl > 1) {
+            dim3 grd((unsigned)((V + 31) / 32), (unsigned)((nl + 31) / 32));
+            k_transpose<<<grd, 256, 0, g->stream>>>(dist, V, nl, dist_d + g0 * V);
+            GIR_LAUNCH(g, "k_transpose");
+        }
     }
-    GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * 32, cudaMemcpyDeviceToHost, g->stream));
+    GIR_TRY(read());
     GIR_CUDA(g, cudaEventRecord(g->ev1, g->stream));
     GIR_CUDA(g, cudaEventSynchronize(g->ev1));
     st.reached = (int64_t)hc[S_REACHED];

@@ -125,11 +125,20 @@ class DeviceGraph:
         self._ck(dev_lib().gir_dev_has_edges(self._h, int(undirected), ptr(u), ptr(v), len(u), ptr(out)), "has_edges")
         return out.astype(bool)
 
+    @staticmethod
+    def _ids(a):
+        """int32 ids as an array the C ABI can read: numpy (host) or a torch tensor (host or device)."""
+        if hasattr(a, "data_ptr"):
+            assert str(a.dtype) == "torch.int32" and a.is_contiguous()
+            return a, int(a.numel())
+        a = np.ascontiguousarray(a, np.int32)
+        return a, len(a)
+
     def bfs(self, sources, out=None):
-        s = np.ascontiguousarray(sources, np.int32)
+        s, n = self._ids(sources)
         if out is None:
-            out = np.empty((len(s), self.V), np.int32)
-        self._ck(dev_lib().gir_dev_bfs(self._h, ptr(s), len(s), ptr(out)), "bfs")
+            out = np.empty((n, self.V), np.int32)
+        self._ck(dev_lib().gir_dev_bfs(self._h, ptr(s), n, ptr(out)), "bfs")
         return out
 
     def bfs_sets(self, sets, out=None):
@@ -142,10 +151,10 @@ class DeviceGraph:
         return out
 
     def sssp(self, sources, delta=16, weights=native.WEIGHT_HASH, out=None):
-        s = np.ascontiguousarray(sources, np.int32)
+        s, n = self._ids(sources)
         if out is None:
-            out = np.empty((len(s), self.V), np.uint64)
-        self._ck(dev_lib().gir_dev_sssp(self._h, ptr(s), len(s), int(delta), weights, ptr(out)), "sssp")
+            out = np.empty((n, self.V), np.uint64)
+        self._ck(dev_lib().gir_dev_sssp(self._h, ptr(s), n, int(delta), weights, ptr(out)), "sssp")
         return out
 
     def sssp_sets(self, sets, delta=16, weights=native.WEIGHT_HASH, out=None):

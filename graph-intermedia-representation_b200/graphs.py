@@ -95,6 +95,16 @@ def sources(V, n, seed):
     return out[:n]
 
 
+def sources_with_edges(g, n, seed):
+    """n sources drawn uniformly among the vertices with at least one out-edge (as Graph500
+    draws its search keys), so a query is never trivially empty."""
+    cand = np.nonzero(np.diff(g.fw_beg) > 0)[0].astype(np.int32)
+    if len(cand) == 0:
+        return sources(g.V, n, seed)
+    lib = native.gen_lib()
+    return np.array([cand[lib.gir_gen_hash3(seed, i, 98) % len(cand)] for i in range(n)], np.int32)
+
+
 def updates(g, n_ins, n_del, seed):
     """A batch of n_ins uniform inserts and n_del deletions sampled from g's edges, shuffled."""
     n = n_ins + n_del

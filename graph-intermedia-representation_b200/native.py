@@ -21,7 +21,8 @@ LAYER_WCC, LAYER_SCC, LAYER_BCT, LAYER_ALL = 1, 2, 4, 7
 LABEL_WCC, LABEL_SCC, LABEL_BLOCK, LABEL_BCNT, LABEL_SCC_RANK = 0, 1, 2, 3, 4
 WEIGHT_HASH, WEIGHT_STORED = 0, 1
 SCHEDULE_FIXED, SCHEDULE_LEARNED = 0, 1
-PARAM_ALPHA, PARAM_BETA, PARAM_DELTA, PARAM_BLOCK, PARAM_SMALL_DEG, PARAM_LARGE_DEG, PARAM_CTAS_PER_SM = range(7)
+(PARAM_ALPHA, PARAM_BETA, PARAM_DELTA, PARAM_BLOCK, PARAM_SMALL_DEG, PARAM_LARGE_DEG, PARAM_CTAS_PER_SM,
+ PARAM_PROFILE) = range(8)
 SCHED_IN, SCHED_HID, SCHED_OUT = 8, 32, 8
 
 # Every symbol include/gir_dev.h declares (checked by the CPU test suite).
@@ -49,7 +50,7 @@ class GirError(RuntimeError):
 class QueryStats(ctypes.Structure):
     _fields_ = [("edges", ctypes.c_int64), ("reached", ctypes.c_int64), ("iterations", ctypes.c_int64),
                 ("bottom_up", ctypes.c_int64), ("launches", ctypes.c_int64), ("kernel_ms", ctypes.c_double),
-                ("total_ms", ctypes.c_double)]
+                ("total_ms", ctypes.c_double), ("main_ms", ctypes.c_double), ("main_launches", ctypes.c_int64)]
 
 
 _P = ctypes.c_void_p

@@ -175,7 +175,9 @@ enum {
     GIR_PARAM_SMALL_DEG = 4,    /* degree bin: thread per vertex below this in-degree */
     GIR_PARAM_LARGE_DEG = 5,    /* degree bin: CTA per vertex from this in-degree on */
     GIR_PARAM_CTAS_PER_SM = 6,  /* grid size = SMs x this */
-    GIR_PARAM_COUNT = 7
+    GIR_PARAM_PROFILE = 7,      /* 1: time every launch of the main traversal kernel with CUDA events
+                                   (gir_dev_query_stats main_ms / main_launches); 0: off */
+    GIR_PARAM_COUNT = 8
 };
 int gir_dev_set_param(gir_dev_t* g, int which, double value);
 int gir_dev_get_param(gir_dev_t* g, int which, double* value);
@@ -190,6 +192,9 @@ typedef struct {
     int64_t launches;       /* kernels launched by the call */
     double kernel_ms;       /* device time of the traversal kernels (CUDA events) */
     double total_ms;        /* device time of the whole call including copies */
+    double main_ms;         /* with GIR_PARAM_PROFILE: summed device time of the main kernel's
+                               launches (BFS: expand + bottom-up kernels; SSSP: relax) */
+    int64_t main_launches;  /* ... and their number */
 } gir_dev_query_stats_t;
 int gir_dev_query_stats(gir_dev_t* g, gir_dev_query_stats_t* out);
 

@@ -48,16 +48,38 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="rmat_lj", choices=["rmat_lj", "rmat_s16"])
+    p.add_argument("--workload", default="rmat_lj", choices=["rmat_lj", "rmat_s20", "rmat_s16"])
     p.add_argument("--no-updates", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--only", choices=["bfs", "sssp"], default=None,
+                   help="profiling runs: one call of one query kind, no timing and no JSON line")
     return p.parse_args()
 
 
 def workload(pkg, name):
     if name == "rmat_lj":
         return pkg.graphs.rmat_lj()
+    if name == "rmat_s20":  # 1M vertices, 2^24 draws: a profiling case larger than L2
+        return pkg.graphs.rmat(20, seed=3, permute=True, name="rmat_s20")
     return pkg.graphs.rmat_s16()
+
+
+def run_only(args):
+    """One call of one query kind (64 queries) on cuda:0, for ncu captures."""
+    import torch
+    pkg = importlib.import_module("graph-intermedia-representation_b200")
+    g = workload(pkg, args.workload)
+    d = pkg.DeviceGraph.from_graph(g)
+    src = torch.from_numpy(pkg.graphs.sources_with_edges(g, 64, 11)).to("cuda:0")
+    if args.only == "bfs":
+        out = torch.empty((64, g.V), dtype=torch.int32, device="cuda:0")
+        d.bfs(src, out=out)
+    else:
+        out = torch.empty((64, g.V), dtype=torch.int64, device="cuda:0")
+        d.sssp(src, delta=DELTA, weights=pkg.native.WEIGHT_HASH, out=out)
+    torch.cuda.synchronize()
+    print(json.dumps({"only": args.only, "workload": args.workload, **d.query_stats()}))
+    d.close()
 
 
 def config(name, g):
@@ -352,7 +374,9 @@ def run_ours(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.only:
+        run_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -29,9 +29,9 @@ constexpr uint64_t kInf = ~0ull;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
 // counters: [0] next near queue length, [1] far queue length, [2] settled queue length,
-// [3] min live far distance, [4] far queue length after a split, [8] length of the queue being
-// read; accumulated over the call: [16] reached (vertex, lane) pairs, [17] their out-edges
-enum { S_NEAR = 0, S_FAR = 1, S_SET = 2, S_MIN = 3, S_FAR2 = 4, S_QLEN = 8, S_REACHED = 16, S_EDGES = 17, S_N = 32 };
+// [3] min live far distance, [4] far queue length after a split, [5] relaxation items;
+// accumulated over the call: [16] reached (vertex, lane) pairs, [17] their out-edges
+enum { S_NEAR = 0, S_FAR = 1, S_SET = 2, S_MIN = 3, S_FAR2 = 4, S_ITEMS = 5, S_REACHED = 16, S_EDGES = 17, S_N = 32 };
 
 __global__ void k_ws_keys(int64_t V, int64_t E, const int64_t* cb, CSRView c, int hash, uint64_t* keys,
                           uint32_t* cols) {
@@ -103,90 +103,163 @@ struct Relax {
     unsigned long long* cnt;
 };
 
-// Work-balanced relaxation, in two kernels. k_relax_prep takes every queued vertex's lanes (and
-// clears them), does the settle bookkeeping and stores the vertex's edge range and lane mask with
-// its work (edges x lanes); after an exclusive scan of the work, k_relax_run cuts the whole
-// queue's (edge, lane) pairs into equal chunks, so a hub with many lanes is spread over the grid
-// instead of one warp. Pairs are enumerated edge-major within a vertex: with many lanes active,
-// consecutive threads update consecutive lanes of one distance row.
+// Work-balanced relaxation: k_relax_prep turns the queue into items (one per vertex with work),
+// an exclusive scan of the items' work (edges x lanes) numbers all (edge, lane) pairs, and
+// k_relax_tile processes them in equal tiles, so a hub with many lanes is spread over the grid.
 struct Items {
     int32_t* u;
     int64_t* eb;
     unsigned long long* m;
-    int32_t* pc;
-    int64_t* pref;  // work per entry, then its exclusive scan (n + 1 entries)
+    int64_t* pref;  // work per item, then its exclusive scan (n + 1 entries)
 };
 
-__global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, Items it) {
-    GRID_STRIDE(i, n) {
-        const int32_t u = q[i];
-        unsigned long long m;
-        if (heavy) {
-            m = a.setmask[u];
-            a.setmask[u] = 0ull;
-        } else {
-            m = a.curmask[u];
-            a.curmask[u] = 0ull;
-            if (m && atomicOr(&a.setmask[u], m) == 0ull) a.setq[atomicAdd(&a.cnt[S_SET], 1ull)] = u;
-        }
-        const int pc = __popcll(m);
-        const int64_t b = a.wb[u], e = b + a.wdeg[u];
-        int64_t lo = b, hi = e;  // light edges: the prefix with weight < delta
+// Number of light edges (weight < delta) of every weight-sorted row, once per query group.
+__global__ void k_light_split(int64_t V, const int64_t* wb, const int32_t* wdeg, const uint32_t* ww, uint64_t delta,
+                              int32_t* nlight) {
+    GRID_STRIDE(v, V) {
+        const int64_t b = wb[v], e = b + wdeg[v];
+        int64_t lo = b, hi = e;
         while (lo < hi) {
             const int64_t mid = (lo + hi) >> 1;
-            if ((uint64_t)a.ww[mid] < a.delta) lo = mid + 1; else hi = mid;
+            if ((uint64_t)ww[mid] < delta) lo = mid + 1; else hi = mid;
         }
-        it.u[i] = u;
-        it.eb[i] = heavy ? lo : b;
-        it.m[i] = m;
-        it.pc[i] = pc;
-        it.pref[i] = (heavy ? e - lo : lo - b) * pc;
+        nlight[v] = (int32_t)(lo - b);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) it.pref[n] = 0;
 }
 
-constexpr int kChunk = 32 * 8;  // (edge, lane) pairs per warp chunk
-
-__global__ void __launch_bounds__(kBlock) k_relax_run(int64_t n, Items it, Relax a) {
-    const int64_t total = it.pref[n];  // (after the scan: all pairs of the queue)
-    const int lane = lane_id();
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c0 = warp * kChunk; c0 < total; c0 += nwarps * kChunk) {
-        const int64_t c1 = c0 + kChunk < total ? c0 + kChunk : total;
-        const int64_t key = c0 + lane < total ? c0 + lane : total - 1;
-        int64_t lo = 0, hi = n - 1;  // entry owning this lane's first pair
-        while (lo < hi) {
-            const int64_t mid = (lo + hi + 1) >> 1;
-            if (it.pref[mid] <= key) lo = mid; else hi = mid - 1;
+// Takes every queued vertex's lanes (clearing them), does the settle bookkeeping and appends an
+// item (vertex, first edge, lane mask, work = edges x lanes) for every vertex with work; the
+// item count goes to cnt[S_ITEMS].
+__global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, const int32_t* nlight, Items it) {
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        int32_t u = 0;
+        unsigned long long m = 0;
+        int64_t eb = 0, work = 0;
+        if (i < n) {
+            u = q[i];
+            if (heavy) {
+                m = a.setmask[u];
+                a.setmask[u] = 0ull;
+            } else {
+                m = a.curmask[u];
+                a.curmask[u] = 0ull;
+                if (m && atomicOr(&a.setmask[u], m) == 0ull) a.setq[atomicAdd(&a.cnt[S_SET], 1ull)] = u;
+            }
+            const int64_t b = a.wb[u];
+            const int32_t nlu = nlight[u];
+            eb = heavy ? b + nlu : b;
+            work = (int64_t)(heavy ? a.wdeg[u] - nlu : nlu) * __popcll(m);
         }
-        int64_t i = lo;
-        for (int64_t base = c0; base < c1; base += 32) {  // warp-uniform
-            const int64_t p = base + lane;
+        const bool has = work > 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, has);
+        if (bal) {
+            const int leader = __ffs(bal) - 1;
+            unsigned long long slot = 0;
+            if (lane_id() == leader) slot = atomicAdd(&a.cnt[S_ITEMS], (unsigned long long)__popc(bal));
+            slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(bal & ((1u << lane_id()) - 1));
+            if (has) {
+                it.u[slot] = u;
+                it.eb[slot] = eb;
+                it.m[slot] = m;
+                it.pref[slot] = work;
+            }
+        }
+    }
+}
+
+constexpr int kTileThreads = 256;
+constexpr int kPairs = 4;                          // pairs in flight per thread
+constexpr int kTile = kTileThreads * kPairs;       // (edge, lane) pairs per CTA tile
+
+// Load-balanced relaxation: CTA tiles of kTile consecutive pairs of the whole item list. The
+// items overlapping a tile (at most kTile, every item has work) are staged in shared memory;
+// each pair finds its item by binary search there, so no thread walks item boundaries through
+// global memory. Pairs are enumerated edge-major within an item: with many lanes active,
+// consecutive threads update consecutive lanes of one distance row.
+__global__ void __launch_bounds__(kTileThreads) k_relax_tile(const unsigned long long* n_items, Items it, Relax a) {
+    __shared__ int32_t s_off[kTile + 1];            // item start, relative to the tile start
+    __shared__ int64_t s_eb[kTile];
+    __shared__ unsigned long long s_m[kTile];
+    __shared__ int32_t s_u[kTile];
+    __shared__ int64_t s_range[2];
+    const int64_t n = (int64_t)*n_items;
+    if (n == 0) return;
+    const int64_t total = it.pref[n];
+    for (int64_t t0 = (int64_t)blockIdx.x * kTile; t0 < total; t0 += (int64_t)gridDim.x * kTile) {
+        const int64_t t1 = t0 + kTile < total ? t0 + kTile : total;
+        if (threadIdx.x < 2) {  // items holding the tile's first and last pair
+            const int64_t key = threadIdx.x == 0 ? t0 : t1 - 1;
+            int64_t lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi + 1) >> 1;
+                if (it.pref[mid] <= key) lo = mid; else hi = mid - 1;
+            }
+            s_range[threadIdx.x] = lo;
+        }
+        __syncthreads();
+        const int64_t e0 = s_range[0];
+        const int ne = (int)(s_range[1] - e0 + 1);
+        for (int j = threadIdx.x; j < ne; j += kTileThreads) {
+            const int64_t e = e0 + j;
+            s_off[j] = (int32_t)(it.pref[e] - t0);  // (the first item may start before the tile)
+            s_eb[j] = it.eb[e];
+            s_m[j] = it.m[e];
+            s_u[j] = it.u[e];
+        }
+        if (threadIdx.x == 0) s_off[ne] = (int32_t)(it.pref[s_range[1] + 1] - t0);
+        __syncthreads();
+        int32_t w[kPairs], s[kPairs];
+        int64_t k[kPairs];
+        uint64_t du[kPairs];
+        bool on[kPairs];
+#pragma unroll
+        for (int j = 0; j < kPairs; ++j) {
+            const int64_t p = t0 + j * kTileThreads + threadIdx.x;
+            on[j] = p < t1;
+            if (on[j]) {
+                const int32_t rel = (int32_t)(p - t0);
+                int lo = 0, hi = ne - 1;  // item: largest x with s_off[x] <= rel
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_off[mid] <= rel) lo = mid; else hi = mid - 1;
+                }
+                const unsigned long long m = s_m[lo];
+                const int pc = __popcll(m);
+                const int32_t q2 = rel - s_off[lo];
+                k[j] = s_eb[lo] + q2 / pc;
+                s[j] = nth_bit(m, q2 % pc);
+                du[j] = a.dist[(int64_t)s_u[lo] * a.nl + s[j]];
+            }
+        }
+        uint32_t wt[kPairs];
+#pragma unroll
+        for (int j = 0; j < kPairs; ++j) {
+            if (on[j]) { w[j] = a.wadj[k[j]]; wt[j] = a.ww[k[j]]; } else { w[j] = 0; wt[j] = 0; }
+        }
+        uint64_t cur[kPairs];
+#pragma unroll
+        for (int j = 0; j < kPairs; ++j)
+            cur[j] = on[j] ? *(volatile uint64_t*)&a.dist[(int64_t)w[j] * a.nl + s[j]] : 0ull;
+#pragma unroll
+        for (int j = 0; j < kPairs; ++j) {
             bool to_near = false, to_far = false;
-            int32_t w = 0;
-            if (p < c1) {
-                while (it.pref[i + 1] <= p) ++i;
-                const int32_t q2 = (int32_t)(p - it.pref[i]);
-                const int pcl = it.pc[i];
-                const int64_t k = it.eb[i] + q2 / pcl;
-                const int s = nth_bit(it.m[i], q2 % pcl);
-                const int32_t uu = it.u[i];
-                w = a.wadj[k];
-                const uint64_t nd = a.dist[(int64_t)uu * a.nl + s] + (uint64_t)a.ww[k];
-                uint64_t* dw = &a.dist[(int64_t)w * a.nl + s];
-                if (nd < *(volatile uint64_t*)dw) {  // plain pre-check: most relaxations lose
-                    const unsigned long long old = atomicMin((unsigned long long*)dw, (unsigned long long)nd);
+            if (on[j]) {
+                const uint64_t nd = du[j] + (uint64_t)wt[j];
+                if (nd < cur[j]) {  // plain pre-check: most relaxations lose
+                    const unsigned long long old =
+                        atomicMin((unsigned long long*)&a.dist[(int64_t)w[j] * a.nl + s[j]], (unsigned long long)nd);
                     if (nd < old) {
-                        const unsigned long long bit = 1ull << s;
-                        if (nd < a.kend) to_near = atomicOr(&a.nextmask[w], bit) == 0ull;
-                        else to_far = atomicOr(&a.farmask[w], bit) == 0ull;
+                        const unsigned long long bit = 1ull << s[j];
+                        if (nd < a.kend) to_near = atomicOr(&a.nextmask[w[j]], bit) == 0ull;
+                        else to_far = atomicOr(&a.farmask[w[j]], bit) == 0ull;
                     }
                 }
             }
-            warp_append(to_near, w, a.nextq, &a.cnt[S_NEAR]);
-            warp_append(to_far, w, a.farq, &a.cnt[S_FAR]);
+            warp_append(to_near, w[j], a.nextq, &a.cnt[S_NEAR]);
+            warp_append(to_far, w[j], a.farq, &a.cnt[S_FAR]);
         }
+        __syncthreads();  // (the next tile overwrites the staged items)
     }
 }
 
@@ -357,11 +430,14 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
     };
     const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
     MainTimer timer{g, g->params[GIR_PARAM_PROFILE] != 0.0};
+    // the relaxation is latency-bound: a full SM's worth of warps (8 CTAs x 256 threads) hides it
+    const int run_grid = g->num_sms * 8;
+    int32_t* nlight = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[9], V + 1, &nlight));
     Items items;
     GIR_TRY(ensure_n(g, g->qitems[0], V + 1, &items.u));
     GIR_TRY(ensure_n(g, g->qitems[1], V + 1, &items.eb));
     GIR_TRY(ensure_n(g, g->qitems[2], V + 1, &items.m));
-    GIR_TRY(ensure_n(g, g->qitems[3], V + 1, &items.pc));
     GIR_TRY(ensure_n(g, g->qitems[4], V + 2, &items.pref));
     GIR_CUDA(g, cudaEventRecord(g->ev0, g->stream));
     GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * S_N, g->stream));
@@ -403,16 +479,24 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         a.farmask = farmask; a.setmask = setmask; a.setq = setq; a.cnt = cnt;
         uint64_t k = 0;
         // one relaxation pass over queue q (n entries): prep, scan of the work, balanced run
+        k_light_split<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, ws.beg, ws.deg, ws.w, D, nlight);
+        GIR_LAUNCH(g, "k_light_split");
         auto relax = [&](const int32_t* q, int64_t n, int heavy) -> int {
-            k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, items);
+            GIR_CUDA(g, cudaMemsetAsync(cnt + S_ITEMS, 0, sizeof(unsigned long long), g->stream));
+            k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, nlight, items);
             GIR_LAUNCH(g, "k_relax_prep");
-            GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));
+            GIR_TRY(read());
+            const int64_t ni = (int64_t)hc[S_ITEMS];
+            st.launches++;
+            if (ni == 0) return GIR_OK;
+            GIR_CUDA(g, cudaMemsetAsync(items.pref + ni, 0, sizeof(int64_t), g->stream));
+            GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, ni + 1));
             GIR_TRY(timer.run([&]() -> int {
-                k_relax_run<<<grid, kBlock, 0, g->stream>>>(n, items, a);
-                GIR_LAUNCH(g, "k_relax_run");
+                k_relax_tile<<<run_grid, kTileThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
+                GIR_LAUNCH(g, "k_relax_tile");
                 return GIR_OK;
             }));
-            st.launches += 4;  // prep, the scan's two kernels, run
+            st.launches += 3;  // the scan's two kernels, the tile kernel
             return GIR_OK;
         };
         while (true) {

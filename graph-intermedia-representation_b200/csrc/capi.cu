@@ -14,7 +14,7 @@ namespace gir {
 namespace {
 
 constexpr int kBlock = 256;
-thread_local std::string g_create_err;
+thread_local std::string g_create_err;  // last failure of a call without a handle
 
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
@@ -445,6 +445,9 @@ int query_sets(gir_dev* g, const int64_t* set_beg_user, const int32_t* srcs, int
 }
 
 }  // namespace
+
+void set_thread_error(const std::string& msg) { g_create_err = msg; }
+
 }  // namespace gir
 
 using namespace gir;

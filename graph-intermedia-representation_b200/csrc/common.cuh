@@ -137,6 +137,8 @@ namespace gir {
 
 // Records an error on the handle and returns `code`.
 int fail(gir_dev* g, int code, const std::string& msg);
+// The text gir_dev_last_error(NULL) returns on this thread (calls that have no handle).
+void set_thread_error(const std::string& msg);
 // Checks a CUDA result; on failure records it and returns GIR_ERR_CUDA (or GIR_ERR_OOM).
 int cuda_check(gir_dev* g, cudaError_t e, const char* what);
 #define GIR_CUDA(g, call) GIR_TRY(::gir::cuda_check((g), (call), #call))

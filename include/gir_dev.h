@@ -201,6 +201,24 @@ int gir_dev_query_stats(gir_dev_t* g, gir_dev_query_stats_t* out);
 /* The CUDA stream of the handle (a cudaStream_t), for callers that time or order work on it. */
 int gir_dev_stream(gir_dev_t* g, void** stream);
 
+/* ---- BFS without allocation ----
+ *
+ * No counterpart in the reference: an entry point for callers that cannot allocate memory at
+ * call time -- a host engine that gives all of a GPU's memory to its own arena, or a
+ * latency-critical thread that cannot afford a cudaMalloc / cudaFree (they can synchronize the
+ * whole device). It computes the BFS levels of GIR::bfs (gir_query.cpp:108-294) from one source
+ * over the caller's compact CSR: beg int64[V+1], adj int32[beg[V]] and level_out int32[V], all in
+ * device memory of the current device; `stream` is a cudaStream_t (NULL: the default stream).
+ * It allocates nothing: its working memory is a static device array sized for at most
+ * GIR_NOALLOC_MAX_V vertices (16 MiB, held by every GPU that loads the library until exit);
+ * larger V gives GIR_ERR_CAPACITY, a malformed CSR GIR_ERR_MALFORMED (text in
+ * gir_dev_last_error(NULL)). The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress): make that first call before any stream capture. All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race. */
+#define GIR_NOALLOC_MAX_V (1 << 21)
+int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64_t V, int32_t source, int32_t* level_out,
+                        void* stream);
+
 /* ---- learned schedule (north-star "learned part") ---- */
 
 /* Schedule network: a 2-layer MLP (GIR_SCHED_IN features -> GIR_SCHED_HID tanh -> GIR_SCHED_OUT

@@ -290,6 +290,8 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
     const int64_t V = g->V;
     QueryStats& st = g->qstats;
     st = QueryStats{};
+    g->trace_x.clear();
+    g->trace_y.clear();
     if (n_sets <= 0) return GIR_OK;
     GIR_CUDA(g, cudaMemsetAsync(level_d, 0xff, sizeof(int32_t) * V * n_sets, g->stream));
     if (V == 0) return GIR_OK;
@@ -355,10 +357,9 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
         while (nq > 0) {
             // direction (the reference's switch, gir_query.cpp:159-169, or the schedule network)
             if (V >= 4096) {
+                float feat[GIR_SCHED_IN];
+                sched_bfs_features(g, nf, mf, mu, L, bottom_up, nl, feat);
                 if (g->schedule == GIR_SCHEDULE_LEARNED && g->sched_loaded) {
-                    float feat[GIR_SCHED_IN] = {(float)(nf / V), (float)(mf / (E + 1.0)), (float)(mu / (E + 1.0)),
-                                                (float)((double)L / 64.0), bottom_up ? 1.f : 0.f,
-                                                (float)((double)E / V / 64.0), (float)(nl / 64.0), 1.f};
                     int bu = bottom_up;
                     GIR_TRY(sched_choose_direction(g, feat, bottom_up, &bu));
                     bottom_up = bu != 0;
@@ -366,6 +367,7 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
                     if (!bottom_up && mf * alpha > mu) bottom_up = true;
                     else if (bottom_up && nf * beta < (double)V) bottom_up = false;
                 }
+                sched_trace(g, feat, bottom_up ? 1 : 0);
             }
             GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
             if (!bottom_up) {

@@ -130,6 +130,9 @@ struct gir_dev {
     std::vector<float> sched_host;    // host copy of the MLP parameters
 
     gir::QueryStats qstats;
+    std::vector<float> trace_x;       // schedule features of the last query call, GIR_SCHED_IN per row
+    std::vector<int32_t> trace_y;     // the class taken for each row
+    double wstat[2][2] = {{0, 0}, {0, 0}};  // per weight mode: mean and max weight (set with ws)
     std::string err;
 };
 
@@ -221,6 +224,15 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
 // ---- schedule network (sched.cu) ----
 int sched_choose_delta(gir_dev* g, const float* features, uint64_t* delta);
 int sched_choose_direction(gir_dev* g, const float* features, int current, int* bottom_up);
+// Feature rows (GIR_SCHED_IN floats) of the two decisions. BFS level: frontier vertices and
+// out-edges, unexplored out-edges, level, current direction, graph density, lanes. SSSP group:
+// density, mean / max weight, size, lanes.
+void sched_bfs_features(const gir_dev* g, double nf, double mf, double mu, int level, bool bottom_up, int lanes,
+                        float* out);
+void sched_sssp_features(const gir_dev* g, int weight_mode, int lanes, float* out);
+// Class of a Delta value among the candidates (nearest in log scale).
+int sched_delta_class(uint64_t delta);
+void sched_trace(gir_dev* g, const float* x, int32_t y);
 
 // ---------------------------------------------------------------------------------------------
 // Device helpers

@@ -1,2 +1,225 @@
-// C++ GIR class over the gir_dev C ABI (placeholder until the class lands).
+// The C++ GIR class (include/gir_b200.hpp) over the gir_dev_* C ABI.
 #include "gir_b200.hpp"
+
+#include <algorithm>
+#include <utility>
+
+namespace gir_b200 {
+
+void BlockCutTree::build(const std::vector<std::vector<int>>& blocks, const std::unordered_set<int>& aps) {
+    // block_cut_tree.h:31-58: C-nodes first, then one B-node per block linked to its APs
+    nodes.clear();
+    std::map<int, int> ap_node;
+    std::vector<int> ap_sorted(aps.begin(), aps.end());
+    std::sort(ap_sorted.begin(), ap_sorted.end());
+    for (int v : ap_sorted) {
+        ap_node[v] = (int)nodes.size();
+        nodes.push_back({C_NODE, v, {}});
+    }
+    for (size_t i = 0; i < blocks.size(); ++i) {
+        const int b = (int)nodes.size();
+        nodes.push_back({B_NODE, (int)i, {}});
+        for (int x : blocks[i]) {
+            auto it = ap_node.find(x);
+            if (it == ap_node.end()) continue;
+            nodes[b].neighbors.push_back(it->second);
+            nodes[it->second].neighbors.push_back(b);
+        }
+    }
+}
+
+void GIR::check(int rc, const char* what) const {
+    if (rc != GIR_OK) throw Error(rc, std::string(what) + ": " + gir_dev_last_error(h_));
+}
+
+GIR::GIR(gir_dev_t* h) : h_(h) {
+    int64_t V = 0;
+    check(gir_dev_counts(h_, &V, nullptr, nullptr, nullptr, nullptr, nullptr), "gir_dev_counts");
+    V_ = (int)V;
+}
+
+GIR::GIR(const std::string& path_directed, const std::string& /*path_undirected: never read, gir.h:156-158*/) {
+    gir_dev_t* h = nullptr;
+    const int rc = gir_dev_load(path_directed.c_str(), &h);
+    if (rc != GIR_OK) throw Error(rc, std::string("gir_dev_load: ") + gir_dev_last_error(nullptr));
+    h_ = h;
+    int64_t V = 0;
+    check(gir_dev_counts(h_, &V, nullptr, nullptr, nullptr, nullptr, nullptr), "gir_dev_counts");
+    V_ = (int)V;
+}
+
+GIR::GIR(int V, const std::vector<int>& fw_beg, const std::vector<int>& fw_adj, const std::vector<int>& bw_beg,
+         const std::vector<int>& bw_adj, const std::vector<uint32_t>* weights) {
+    if ((int)fw_beg.size() != V + 1 || (int)bw_beg.size() != V + 1 || fw_adj.size() != bw_adj.size() ||
+        (weights && weights->size() != fw_adj.size()))
+        throw Error(GIR_ERR_INVALID, "GIR: CSR arrays of inconsistent sizes");
+    gir_dev_t* h = nullptr;
+    const int rc = gir_dev_create(fw_beg.data(), fw_adj.data(), bw_beg.data(), bw_adj.data(), V,
+                                  (int64_t)fw_adj.size(), weights ? weights->data() : nullptr, &h);
+    if (rc != GIR_OK) throw Error(rc, std::string("gir_dev_create: ") + gir_dev_last_error(nullptr));
+    h_ = h;
+    V_ = V;
+}
+
+GIR GIR::fromEdges(int V, const std::vector<std::pair<int, int>>& edges) {
+    std::vector<int> fb(V + 1, 0), bb(V + 1, 0), fa(edges.size()), ba(edges.size());
+    for (auto& e : edges) { fb[e.first + 1]++; bb[e.second + 1]++; }
+    for (int v = 0; v < V; ++v) { fb[v + 1] += fb[v]; bb[v + 1] += bb[v]; }
+    std::vector<int> fp(fb.begin(), fb.end() - 1), bp(bb.begin(), bb.end() - 1);
+    for (auto& e : edges) { fa[fp[e.first]++] = e.second; ba[bp[e.second]++] = e.first; }
+    return GIR(V, fb, fa, bb, ba);
+}
+
+GIR::GIR(GIR&& o) noexcept : h_(o.h_), V_(o.V_) { o.h_ = nullptr; }
+GIR& GIR::operator=(GIR&& o) noexcept {
+    if (this != &o) {
+        gir_dev_destroy(h_);
+        h_ = o.h_;
+        V_ = o.V_;
+        o.h_ = nullptr;
+    }
+    return *this;
+}
+GIR::~GIR() { gir_dev_destroy(h_); }
+
+void GIR::buildWCC() { check(gir_dev_build(h_, GIR_LAYER_WCC), "buildWCC"); }
+void GIR::buildSCC_DAG() { check(gir_dev_build(h_, GIR_LAYER_SCC), "buildSCC_DAG"); }
+void GIR::buildBCT() { check(gir_dev_build(h_, GIR_LAYER_BCT), "buildBCT"); }
+
+void GIR::applyBatch(const std::vector<Update>& batch) {
+    std::vector<int32_t> u(batch.size()), v(batch.size());
+    std::vector<uint8_t> ins(batch.size());
+    for (size_t i = 0; i < batch.size(); ++i) {
+        u[i] = batch[i].u;
+        v[i] = batch[i].v;
+        ins[i] = batch[i].insert ? 1 : 0;
+    }
+    check(gir_dev_apply_batch(h_, u.data(), v.data(), ins.data(), (int64_t)batch.size()), "applyBatch");
+}
+void GIR::insertEdge(int u, int v) { applyBatch({{u, v, true}}); }
+void GIR::deleteEdge(int u, int v) { applyBatch({{u, v, false}}); }
+void GIR::updateEdgeDirected(int u, int v, bool insert) { applyBatch({{u, v, insert}}); }
+void GIR::updateEdgeUndirected(int u, int v, bool insert) { applyBatch({{u, v, insert}}); }
+
+std::vector<int32_t> GIR::labels(int which) const {
+    std::vector<int32_t> out((size_t)V_);
+    check(gir_dev_get_labels(h_, which, out.data()), "get_labels");
+    return out;
+}
+
+int GIR::sccOf(int v) const { return labels(GIR_LABEL_SCC).at((size_t)v); }
+int GIR::wccOf(int v) const { return labels(GIR_LABEL_WCC).at((size_t)v); }
+long long GIR::sccRank(int s) const { return labels(GIR_LABEL_SCC_RANK).at((size_t)s); }
+bool GIR::isArticulationPoint(int v) const { return labels(GIR_LABEL_BCNT).at((size_t)v) >= 2; }
+
+std::map<int, int> GIR::getNodeToScc() const {
+    const auto l = labels(GIR_LABEL_SCC);
+    std::map<int, int> m;
+    for (int v = 0; v < V_; ++v) m.emplace_hint(m.end(), v, l[v]);
+    return m;
+}
+std::map<int, int> GIR::getNodeToWcc() const {
+    const auto l = labels(GIR_LABEL_WCC);
+    std::map<int, int> m;
+    for (int v = 0; v < V_; ++v) m.emplace_hint(m.end(), v, l[v]);
+    return m;
+}
+std::vector<std::vector<int>> GIR::getSCCs() const {
+    const auto l = labels(GIR_LABEL_SCC);
+    std::vector<std::vector<int>> r((size_t)V_);
+    for (int v = 0; v < V_; ++v) r[l[v]].push_back(v);
+    return r;
+}
+std::vector<std::vector<int>> GIR::getWCCs() const {
+    const auto l = labels(GIR_LABEL_WCC);
+    std::vector<std::vector<int>> byid((size_t)V_), r;
+    for (int v = 0; v < V_; ++v) byid[l[v]].push_back(v);
+    for (auto& g : byid) if (!g.empty()) r.push_back(std::move(g));
+    return r;
+}
+std::vector<std::vector<int>> GIR::getDAG() const {
+    int64_t n = 0;
+    check(gir_dev_get_dag(h_, nullptr, nullptr, 0, &n), "getDAG");
+    std::vector<int32_t> a((size_t)n), b((size_t)n);
+    if (n) check(gir_dev_get_dag(h_, a.data(), b.data(), n, &n), "getDAG");
+    std::vector<std::vector<int>> r((size_t)V_);
+    for (int64_t i = 0; i < n; ++i) r[a[i]].push_back(b[i]);
+    return r;
+}
+std::vector<std::vector<int>> GIR::getBCTComponents(int scc_id) const {
+    const auto scc = labels(GIR_LABEL_SCC);
+    const auto blk = labels(GIR_LABEL_BLOCK);
+    int64_t nb = 0;
+    check(gir_dev_get_blocks(h_, nullptr, 0, &nb), "getBCTComponents");
+    std::vector<int32_t> head((size_t)nb);
+    if (nb) check(gir_dev_get_blocks(h_, head.data(), nb, &nb), "getBCTComponents");
+    std::map<int, std::vector<int>> by_block;
+    for (int v = 0; v < V_; ++v)
+        if (scc[v] == scc_id) by_block[blk[v]].push_back(v);
+    std::vector<std::vector<int>> r;
+    for (auto& kv : by_block) {
+        auto members = kv.second;
+        if (head[kv.first] >= 0) members.push_back(head[kv.first]);
+        std::sort(members.begin(), members.end());
+        r.push_back(std::move(members));
+    }
+    return r;
+}
+BlockCutTree* GIR::getBCT(int scc_id) const {
+    const auto comps = getBCTComponents(scc_id);
+    const auto cnt = labels(GIR_LABEL_BCNT);
+    std::unordered_set<int> aps;
+    for (auto& c : comps)
+        for (int x : c)
+            if (cnt[x] >= 2) aps.insert(x);
+    auto* t = new BlockCutTree();
+    t->build(comps, aps);
+    return t;
+}
+
+std::vector<int> GIR::row(int dir, int v) const {
+    if (v < 0 || v >= V_) return {};
+    int64_t n = 0;
+    check(gir_dev_get_csr(h_, dir, nullptr, nullptr, 0, &n), "get_csr");
+    std::vector<int64_t> beg((size_t)V_ + 1);
+    std::vector<int32_t> adj((size_t)n);
+    check(gir_dev_get_csr(h_, dir, beg.data(), adj.data(), n, &n), "get_csr");
+    return std::vector<int>(adj.begin() + beg[v], adj.begin() + beg[v + 1]);
+}
+std::vector<int> GIR::getDirectedOutNeighbors(int v) const { return row(0, v); }
+std::vector<int> GIR::getDirectedInNeighbors(int v) const { return row(1, v); }
+std::vector<int> GIR::getUndirectedNeighborsPublic(int v) const { return row(2, v); }
+
+bool GIR::hasDirectedEdge(int u, int v) const {
+    uint8_t out = 0;
+    check(gir_dev_has_edges(h_, 0, &u, &v, 1, &out), "hasDirectedEdge");
+    return out != 0;
+}
+bool GIR::hasUndirectedEdge(int u, int v) const {
+    uint8_t out = 0;
+    check(gir_dev_has_edges(h_, 1, &u, &v, 1, &out), "hasUndirectedEdge");
+    return out != 0;
+}
+
+std::vector<int> GIR::bfs(int source) { return bfsMany({source}); }
+std::vector<uint64_t> GIR::sssp(int source, uint64_t delta) { return ssspMany({source}, delta); }
+
+std::vector<int> GIR::bfsMany(const std::vector<int>& sources) {
+    std::vector<int> out(sources.size() * (size_t)V_);
+    check(gir_dev_bfs(h_, sources.data(), (int64_t)sources.size(), out.data()), "bfs");
+    return out;
+}
+std::vector<uint64_t> GIR::ssspMany(const std::vector<int>& sources, uint64_t delta) {
+    std::vector<uint64_t> out(sources.size() * (size_t)V_);
+    check(gir_dev_sssp(h_, sources.data(), (int64_t)sources.size(), delta, GIR_WEIGHT_HASH, out.data()), "sssp");
+    return out;
+}
+
+uint32_t GIR::edgeWeight(int u, int v) {
+    // GIR::edgeWeight (gir_query.cpp:50-54); the device kernels compute the same function
+    uint64_t x = ((uint64_t)(uint32_t)u << 32) | (uint32_t)v;
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdULL; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
+    return 1 + (uint32_t)(x % kMaxWeight);
+}
+
+}  // namespace gir_b200

@@ -21,7 +21,7 @@ namespace {
 constexpr int IN = GIR_SCHED_IN, HID = GIR_SCHED_HID, OUT = GIR_SCHED_OUT;
 constexpr int NP = HID * IN + HID + OUT * HID + OUT;
 constexpr int kBlock = 128;
-constexpr uint64_t kDeltaChoices[6] = {8, 16, 32, 64, 128, 256};
+constexpr uint64_t kDeltaChoices[6] = {16, 32, 64, 128, 512, 2048};
 
 struct Layout {
     const float *W1, *b1, *W2, *b2;
@@ -166,6 +166,48 @@ int decide(gir_dev* g, const float* features, int lo, int hi, int* choice) {
 
 }  // namespace
 
+void sched_bfs_features(const gir_dev* g, double nf, double mf, double mu, int level, bool bottom_up, int lanes,
+                        float* out) {
+    const double V = (double)(g->V > 0 ? g->V : 1), E = (double)g->fw.E + 1.0;
+    out[0] = (float)(nf / V);
+    out[1] = (float)(mf / E);
+    out[2] = (float)(mu / E);
+    out[3] = (float)((level < 64 ? level : 64) / 64.0);
+    out[4] = bottom_up ? 1.f : 0.f;
+    out[5] = (float)(std::log2(E / V + 1.0) / 8.0);
+    out[6] = (float)(lanes / 64.0);
+    out[7] = 0.f;  // task: BFS direction
+}
+
+void sched_sssp_features(const gir_dev* g, int weight_mode, int lanes, float* out) {
+    const double V = (double)(g->V > 0 ? g->V : 1), E = (double)g->fw.E + 1.0;
+    const int m = weight_mode == GIR_WEIGHT_HASH ? 0 : 1;
+    out[0] = (float)(std::log2(E / V + 1.0) / 8.0);
+    out[1] = (float)(std::log2(g->wstat[m][0] + 1.0) / 16.0);
+    out[2] = (float)(std::log2(g->wstat[m][1] + 1.0) / 16.0);
+    out[3] = (float)(std::log2(V) / 32.0);
+    out[4] = (float)(lanes / 64.0);
+    out[5] = 0.f;
+    out[6] = 0.f;
+    out[7] = 1.f;  // task: SSSP bucket width
+}
+
+int sched_delta_class(uint64_t delta) {
+    int best = 0;
+    double bd = 1e300;
+    for (int i = 0; i < 6; ++i) {
+        const double d = std::fabs(std::log2((double)delta) - std::log2((double)kDeltaChoices[i]));
+        if (d < bd) { bd = d; best = i; }
+    }
+    return 2 + best;
+}
+
+void sched_trace(gir_dev* g, const float* x, int32_t y) {
+    if (g->trace_y.size() >= (1u << 20)) return;  // bounded
+    g->trace_x.insert(g->trace_x.end(), x, x + IN);
+    g->trace_y.push_back(y);
+}
+
 int sched_choose_direction(gir_dev* g, const float* features, int current, int* bottom_up) {
     (void)current;
     int c = 0;
@@ -188,6 +230,24 @@ using namespace gir;
 extern "C" {
 
 int64_t gir_dev_sched_param_count(void) { return NP; }
+
+int gir_dev_sched_delta_choices(uint64_t* out6) {
+    if (!out6) return GIR_ERR_INVALID;
+    for (int i = 0; i < 6; ++i) out6[i] = kDeltaChoices[i];
+    return GIR_OK;
+}
+
+int gir_dev_sched_trace(gir_dev_t* g, float* features, int32_t* choice, int64_t cap, int64_t* n) {
+    if (!g || !n || cap < 0) return GIR_ERR_INVALID;
+    *n = (int64_t)g->trace_y.size();
+    const int64_t m = cap < *n ? cap : *n;
+    if (m > 0 && (!features || !choice)) return fail(g, GIR_ERR_INVALID, "sched_trace: null output");
+    for (int64_t i = 0; i < m; ++i) {
+        for (int k = 0; k < IN; ++k) features[i * IN + k] = g->trace_x[(size_t)i * IN + k];
+        choice[i] = g->trace_y[(size_t)i];
+    }
+    return GIR_OK;
+}
 
 int gir_dev_sched_set_weights(gir_dev_t* g, const float* params, int64_t n_params) {
     if (!g) return GIR_ERR_INVALID;

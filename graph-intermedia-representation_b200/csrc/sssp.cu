@@ -57,6 +57,24 @@ __global__ void k_ws_split(int64_t E, const uint64_t* keys, const uint32_t* cols
     }
 }
 
+// Sum and maximum of the weights (st[0], st[1]).
+__global__ void k_wstat(const uint32_t* w, int64_t E, unsigned long long* st) {
+    unsigned long long s = 0, m = 0;
+    GRID_STRIDE(i, E) {
+        s += w[i];
+        m = w[i] > m ? w[i] : m;
+    }
+    for (int o = 16; o; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t > m ? t : m;
+    }
+    if (lane_id() == 0) {
+        atomicAdd(&st[0], s);
+        atomicMax(&st[1], m);
+    }
+}
+
 __global__ void k_deg_i64(int64_t V, const int32_t* deg, int64_t* out) {
     GRID_STRIDE(v, V) out[v] = deg[v];
     if (blockIdx.x == 0 && threadIdx.x == 0) out[V] = 0;
@@ -381,6 +399,16 @@ static int build_weight_sorted(gir_dev* g, int hash, DevCSR& ws) {
     GIR_TRY(sort_pairs_u64(g, keys, ktmp, cols, ctmp, E, 64));
     k_ws_split<<<grid_for(g, E, kBlock), kBlock, 0, g->stream>>>(E, keys, cols, ws.adj, ws.w);
     GIR_LAUNCH(g, "k_ws_split");
+    // weight statistics for the schedule's features
+    unsigned long long* st = reinterpret_cast<unsigned long long*>(ktmp);
+    GIR_CUDA(g, cudaMemsetAsync(st, 0, 2 * sizeof(unsigned long long), g->stream));
+    k_wstat<<<grid_for(g, E, kBlock), kBlock, 0, g->stream>>>(ws.w, E, st);
+    GIR_LAUNCH(g, "k_wstat");
+    unsigned long long h[2] = {0, 0};
+    GIR_CUDA(g, cudaMemcpyAsync(h, st, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    g->wstat[hash ? 0 : 1][0] = (double)h[0] / (double)E;
+    g->wstat[hash ? 0 : 1][1] = (double)h[1];
     return GIR_OK;
 }
 
@@ -389,6 +417,8 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
     const int64_t V = g->V;
     QueryStats& st = g->qstats;
     st = QueryStats{};
+    g->trace_x.clear();
+    g->trace_y.clear();
     if (n_sets <= 0) return GIR_OK;
     GIR_CUDA(g, cudaMemsetAsync(dist_d, 0xff, sizeof(uint64_t) * V * n_sets, g->stream));
     if (V == 0) return GIR_OK;
@@ -451,17 +481,17 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         uint64_t* dist = nl > 1 ? idist : dist_d + g0 * V;
         if (nl > 1) GIR_CUDA(g, cudaMemsetAsync(dist, 0xff, sizeof(uint64_t) * V * nl, g->stream));
         uint64_t D = delta;
+        float feat[GIR_SCHED_IN];
+        sched_sssp_features(g, weight_mode, nl, feat);
         if (D == 0) {
             if (g->schedule == GIR_SCHEDULE_LEARNED && g->sched_loaded) {
-                const double E = (double)g->fw.E;
-                float feat[GIR_SCHED_IN] = {(float)(E / V / 64.0), hash ? 0.5f : 1.f, (float)(g->num_sms / 148.0),
-                                            (float)(nl / 64.0), 0.f, 0.f, 0.f, 1.f};
                 GIR_TRY(sched_choose_delta(g, feat, &D));
             } else {
                 D = (uint64_t)g->params[GIR_PARAM_DELTA];
             }
             if (D == 0) D = 16;
         }
+        sched_trace(g, feat, sched_delta_class(D));
         GIR_CUDA(g, cudaMemcpyAsync(sbeg, set_beg_h + g0, sizeof(int64_t) * (nl + 1), cudaMemcpyHostToDevice, g->stream));
         for (int k = 0; k < S_N; ++k)
             if (k != S_REACHED && k != S_EDGES) hc[k] = 0;

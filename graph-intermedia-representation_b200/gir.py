@@ -230,6 +230,31 @@ class DeviceGraph:
                  "sched_grad")
         return grad, loss.value
 
+    def use_learned_schedule(self, path=None):
+        """Loads the trained schedule network (schedule_weights.npy, written by
+        train_schedule.py) and switches the traversal choices to it."""
+        import os
+        path = path or os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedule_weights.npy")
+        self.sched_set_weights(np.load(path))
+        self.set_schedule(native.SCHEDULE_LEARNED)
+
+    def sched_trace(self):
+        """(features[n][8], class[n]) of the schedule decisions of the last query call."""
+        n = ctypes.c_int64()
+        self._ck(dev_lib().gir_dev_sched_trace(self._h, None, None, 0, ctypes.byref(n)), "sched_trace")
+        x = np.empty((n.value, native.SCHED_IN), np.float32)
+        y = np.empty(n.value, np.int32)
+        self._ck(dev_lib().gir_dev_sched_trace(self._h, ptr(x), ptr(y), n.value, ctypes.byref(n)), "sched_trace")
+        return x, y
+
+    @staticmethod
+    def delta_choices():
+        out = np.empty(6, np.uint64)
+        rc = dev_lib().gir_dev_sched_delta_choices(ptr(out))
+        if rc != 0:
+            raise GirError(rc, "sched_delta_choices")
+        return out
+
     def sched_train(self, x, y, steps, lr):
         x = np.ascontiguousarray(x, np.float32)
         y = np.ascontiguousarray(y, np.int32)

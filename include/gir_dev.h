@@ -238,6 +238,14 @@ int gir_dev_sched_forward(gir_dev_t* g, const float* x, int64_t n, float* logits
 /* Gradient of the mean cross-entropy w.r.t. all parameters at the current weights. */
 int gir_dev_sched_grad(gir_dev_t* g, const float* x, const int32_t* y, int64_t n, float* grad, float* loss);
 
+/* The schedule decisions of the last query call: one row per BFS level or per SSSP lane group,
+ * features[n][GIR_SCHED_IN] and the class taken (0/1: top-down / bottom-up; 2..7: the Delta
+ * candidates of gir_dev_sched_delta_choices). Writes at most `cap` rows; *n = total. */
+int gir_dev_sched_trace(gir_dev_t* g, float* features, int32_t* choice, int64_t cap, int64_t* n);
+
+/* The six Delta candidates of classes 2..7. */
+int gir_dev_sched_delta_choices(uint64_t* out6);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,60 @@
+// A C++ caller of the GIR class, written the way the reference's drivers use it
+// (gir_constructor/main.cpp:29-52, gir_test.cpp:704-753): load the four-file CSR, build the three
+// layers, run the targeted Case 1 / 5c / 5b updates and a BFS / SSSP, and print what it sees.
+// tests/test_gpu_cpp_class.py compiles it against include/gir_b200.hpp and libgir_b200.so.
+#include <cstdio>
+#include <memory>
+
+#include "gir_b200.hpp"
+
+using GIR = gir_b200::GIR;
+
+static int count_nonempty(const std::vector<std::vector<int>>& parts) {
+    int n = 0;
+    for (auto& p : parts) n += !p.empty();
+    return n;
+}
+
+int main(int argc, char** argv) {
+    if (argc < 2) {
+        std::fprintf(stderr, "usage: %s <dir/>\n", argv[0]);
+        return 2;
+    }
+    try {
+        GIR g(argv[1], argv[1]);
+        g.buildWCC();
+        g.buildSCC_DAG();
+        g.buildBCT();
+        std::printf("V %d\n", g.vertexCount());
+        std::printf("wcc %d scc %d\n", (int)g.getWCCs().size(), count_nonempty(g.getSCCs()));
+        const int w0 = (int)g.getWCCs().size();
+        g.insertEdge(3, 12);  // Case 1: joins two WCCs
+        std::printf("case1 %d\n", (int)g.getWCCs().size() == w0 - 1);
+        g.deleteEdge(3, 12);  // Case 5c: splits them again
+        std::printf("case5c %d\n", (int)g.getWCCs().size() == w0);
+        auto before = g.getNodeToScc();
+        g.updateEdgeUndirected(9, 2, false);  // Case 5b: splits {0,1,2,9,10,11}
+        auto after = g.getNodeToScc();
+        std::printf("case5b %d\n", before[0] == before[9] && after[0] != after[9] && after[0] == after[1] &&
+                                       after[9] == after[10]);
+        auto comps = g.getBCTComponents(g.sccOf(0));
+        std::printf("blocks_of_scc0 %d\n", (int)comps.size());
+        std::unique_ptr<gir_b200::BlockCutTree> t(g.getBCT(g.sccOf(0)));
+        std::printf("bct_nodes %d\n", (int)t->nodes.size());
+        auto lv = g.bfs(0);
+        auto d = g.sssp(0);
+        std::printf("bfs_0_9 %d sssp_0_1 %llu w01 %u\n", lv[9], (unsigned long long)d[1], GIR::edgeWeight(0, 1));
+        std::printf("dag_rows_with_edges %d\n", count_nonempty(g.getDAG()));
+        std::printf("has %d %d %d\n", g.hasDirectedEdge(2, 9), g.hasDirectedEdge(9, 2), g.hasUndirectedEdge(9, 2));
+        try {
+            GIR bad("/nonexistent/dir/", "/nonexistent/dir/");
+            std::printf("error_missing 0\n");
+        } catch (const gir_b200::Error& e) {
+            std::printf("error_missing %d\n", e.code() == GIR_ERR_FILE);
+        }
+    } catch (const gir_b200::Error& e) {
+        std::fprintf(stderr, "error %d: %s\n", e.code(), e.what());
+        return 1;
+    }
+    return 0;
+}

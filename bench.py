@@ -51,8 +51,9 @@ def parse():
     p.add_argument("--workload", default="rmat_lj", choices=["rmat_lj", "rmat_s20", "rmat_s16"])
     p.add_argument("--no-updates", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--only", choices=["bfs", "sssp"], default=None,
-                   help="profiling runs: one call of one query kind, no timing and no JSON line")
+    p.add_argument("--only", choices=["bfs", "sssp", "build"], default=None,
+                   help="profiling runs: one call of one query kind (or the three layer builds and one "
+                        "10K update batch), no timing and no JSON line")
     return p.parse_args()
 
 
@@ -71,6 +72,14 @@ def run_only(args):
     g = workload(pkg, args.workload)
     d = pkg.DeviceGraph.from_graph(g)
     src = torch.from_numpy(pkg.graphs.sources_with_edges(g, 64, 11)).to("cuda:0")
+    if args.only == "build":
+        d.build(pkg.native.LAYER_ALL)
+        u, v, ins = pkg.graphs.updates(g, 5000, 5000, 5)
+        d.apply_batch(u, v, ins)
+        torch.cuda.synchronize()
+        print(json.dumps({"only": "build", "workload": args.workload, **d.counts()}))
+        d.close()
+        return
     if args.only == "bfs":
         out = torch.empty((64, g.V), dtype=torch.int32, device="cuda:0")
         d.bfs(src, out=out)
@@ -349,6 +358,7 @@ def run_ours(args):
             ub, vb, ib = (torch.from_numpy(x).pin_memory() for x in (u, v, ins))
             t = ev_time(lambda: d.apply_batch(ub.numpy(), vb.numpy(), ib.numpy()))
             upd[str(n)] = n / (t * 1e-3)
+            extra.setdefault("update_phases_ms", {})[str(n)] = {k: round(x, 2) for k, x in d.batch_times().items()}
         extra["updates_per_s"] = upd
 
     cpu = None

@@ -37,31 +37,79 @@ struct HView {
     const int32_t* scc;
 };
 
-__global__ void k_roots(int64_t V, const int32_t* scc, int32_t* parent, int32_t* depth, int32_t* order,
-                        unsigned long long* cnt) {
+// SCCs with more than one vertex: every non-smallest member marks its SCC's smallest vertex
+// (plain stores behind a read, so a giant SCC costs a few writes, not one per member).
+__global__ void k_mark_nontrivial(int64_t V, const int32_t* scc, uint8_t* nontrivial) {
+    GRID_STRIDE(v, V) {
+        const int32_t r = scc[v];
+        if (r != (int32_t)v && !nontrivial[r]) nontrivial[r] = 1;
+    }
+}
+
+// Row lengths of H for the sweeps: 0 for the vertices of singleton SCCs (isolated in H).
+__global__ void k_h_deg(int64_t V, const int32_t* scc, const uint8_t* nontrivial, const int32_t* sym_deg,
+                        int32_t* hdeg) {
+    GRID_STRIDE(v, V) hdeg[v] = nontrivial[scc[v]] ? sym_deg[v] : 0;
+}
+
+// Forest roots: every SCC's smallest vertex; only those of non-singleton SCCs start the BFS.
+__global__ void k_roots(int64_t V, const int32_t* scc, const uint8_t* nontrivial, int32_t* parent, int32_t* depth,
+                        int32_t* order, unsigned long long* cnt) {
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t v = base + threadIdx.x;
         bool root = false;
         if (v < V) {
-            root = scc[v] == (int32_t)v;
-            parent[v] = root ? (int32_t)v : -1;
-            depth[v] = root ? 0 : -1;
+            const bool r = scc[v] == (int32_t)v;
+            root = r && nontrivial[v];
+            parent[v] = r ? (int32_t)v : -1;
+            depth[v] = r ? 0 : -1;
         }
         warp_append(root, (int32_t)v, order, &cnt[C_Q]);
     }
 }
 
 // One BFS level of the spanning forest: the level's vertices are order[lo, lo + n); new ones are
-// appended to order after it (the counter starts at lo + n).
-__global__ void __launch_bounds__(kBlock) k_forest_level(const int32_t* level_q, const unsigned long long* qlen,
-                                                         HView h, int32_t* parent, int32_t* depth, int32_t L,
-                                                         int32_t* out, unsigned long long* cnt) {
-    warp_expand(level_q, (int64_t)*qlen, h.sym, out, &cnt[C_Q], [&](int32_t u, int32_t w) {
-        if (h.scc[w] != h.scc[u] || parent[w] != -1) return false;
-        if (atomicCAS(&parent[w], -1, u) != -1) return false;
-        depth[w] = L + 1;
-        return true;
-    });
+// appended to order after it. Edge-balanced: the level's H rows are cut into equal chunks after
+// a scan of their lengths, so hubs of the giant SCC do not serialize a warp.
+__global__ void k_level_deg(const int32_t* q, int64_t n, const int32_t* deg, int64_t* pref) {
+    GRID_STRIDE(i, n) pref[i] = deg[q[i]];
+    if (blockIdx.x == 0 && threadIdx.x == 0) pref[n] = 0;
+}
+
+constexpr int kForestChunk = 32 * 16;
+
+__global__ void __launch_bounds__(kBlock) k_forest_balanced(const int32_t* q, int64_t nq, const int64_t* pref, HView h,
+                                                            int32_t* parent, int32_t* depth, int32_t L, int32_t* out,
+                                                            unsigned long long* cnt) {
+    const int64_t total = pref[nq];
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c0 = warp * kForestChunk; c0 < total; c0 += nwarps * kForestChunk) {
+        const int64_t c1 = c0 + kForestChunk < total ? c0 + kForestChunk : total;
+        const int64_t key = c0 + lane < total ? c0 + lane : total - 1;
+        int64_t lo = 0, hi = nq - 1;
+        while (lo < hi) {
+            const int64_t m = (lo + hi + 1) >> 1;
+            if (pref[m] <= key) lo = m; else hi = m - 1;
+        }
+        int64_t i = lo;
+        for (int64_t base = c0; base < c1; base += 32) {
+            const int64_t p = base + lane;
+            bool push = false;
+            int32_t w = 0;
+            if (p < c1) {
+                while (pref[i + 1] <= p) ++i;
+                const int32_t u = q[i];
+                w = h.sym.adj[h.sym.beg[u] + (p - pref[i])];
+                if (parent[w] == -1 && h.scc[w] == h.scc[u] && atomicCAS(&parent[w], -1, u) == -1) {
+                    depth[w] = L + 1;
+                    push = true;
+                }
+            }
+            warp_append(push, w, out, &cnt[C_Q]);
+        }
+    }
 }
 
 __global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) { GRID_STRIDE(i, n) p[i] = v; }
@@ -114,10 +162,6 @@ __global__ void k_pre_level(const int32_t* q, int64_t n, const int32_t* parent, 
 
 __global__ void k_pre_roots(const int32_t* q, int64_t n, int32_t* pre) { GRID_STRIDE(i, n) pre[q[i]] = 0; }
 
-__device__ __forceinline__ bool is_tree_edge(const int32_t* parent, int32_t u, int32_t w) {
-    return parent[w] == u || parent[u] == w;
-}
-
 // low / high from non-tree edges of H, and rule 1 unions.
 __device__ __forceinline__ int32_t uf_find(int32_t* uf, int32_t x) {
     int32_t p = uf[x];
@@ -140,19 +184,28 @@ __device__ __forceinline__ void uf_union(int32_t* uf, int32_t a, int32_t b, unsi
     atomicAdd(err, 1ull);
 }
 
-__global__ void __launch_bounds__(kBlock) k_nontree(int64_t V, HView h, const int32_t* parent, const int32_t* pre,
-                                                    const int32_t* nd, int32_t* low, int32_t* high, int32_t* uf,
-                                                    unsigned long long* err) {
+// Per-vertex tree data packed for the non-tree sweep: one 16-byte gather per neighbour instead of
+// four scattered 4-byte ones. x = pre, y = nd, z = parent, w = scc.
+__global__ void k_pack_vinfo(int64_t V, const int32_t* pre, const int32_t* nd, const int32_t* parent,
+                             const int32_t* scc, int4* vinfo) {
+    GRID_STRIDE(v, V) vinfo[v] = make_int4(pre[v], nd[v], parent[v], scc[v]);
+}
+
+// One sweep over the non-tree edges of H: low / high of every vertex from its own non-tree
+// neighbours, and rule 1 (once per edge, from its endpoint with the smaller pre) for edges
+// between unrelated endpoints.
+__global__ void __launch_bounds__(kBlock) k_nontree(int64_t V, HView h, const int4* vinfo, int32_t* low, int32_t* high,
+                                                    int32_t* uf, unsigned long long* err) {
     __shared__ int64_t s_excl[kBlock / 32][33];
     __shared__ int32_t s_u[kBlock / 32][32];
     const int wib = threadIdx.x >> 5;
     warp_sweep_rows(h.sym.beg, h.sym.deg, h.sym.adj, 0, V, s_excl[wib], s_u[wib], [&](int32_t u, int32_t w, int64_t) {
-        if (h.scc[u] != h.scc[w] || is_tree_edge(parent, u, w)) return;
-        const int32_t pw = pre[w], pu = pre[u];
-        atomicMin(&low[u], pw);
-        atomicMax(&high[u], pw);
-        // rule 1 (once per edge: from its endpoint with the smaller pre): unrelated endpoints
-        if (pu < pw && pu + nd[u] <= pw) uf_union(uf, u, w, err);
+        const int4 iu = vinfo[u], iw = vinfo[w];
+        if (iu.w != iw.w || iw.z == u || iu.z == w) return;  // other SCC, or a tree edge
+        const int32_t pw = iw.x;
+        if (pw < low[u]) atomicMin(&low[u], pw);  // (plain pre-checks: a hub's row is swept by many
+        if (pw > high[u]) atomicMax(&high[u], pw);  //  threads, most of which change nothing)
+        if (iu.x < pw && iu.x + iu.y <= pw && uf[u] != uf[w]) uf_union(uf, u, w, err);
     });
 }
 
@@ -246,7 +299,7 @@ int bct_build(gir_dev* g) {
     if (!g->scc_built) return fail(g, GIR_ERR_STATE, "buildBCT needs buildSCC_DAG first");
     const int64_t V = g->V;
     const int32_t* scc = static_cast<const int32_t*>(g->scc.p);
-    const HView h{view(g->sym), scc};
+    HView h{view(g->sym), scc};  // (row lengths replaced by the H lengths below)
     int32_t *parent = nullptr, *depth = nullptr, *order = nullptr, *nd = nullptr, *pre = nullptr, *off = nullptr;
     int32_t *low = nullptr, *high = nullptr, *uf = nullptr, *reps = nullptr, *id_of_rep = nullptr;
     uint64_t *keys = nullptr, *ktmp = nullptr;
@@ -268,7 +321,6 @@ int bct_build(gir_dev* g) {
     GIR_TRY(ensure_n(g, g->scratch[12], V + 2, &scan));
     GIR_TRY(ensure_n(g, g->scratch[13], V + 1, &first));
     GIR_TRY(ensure_n(g, g->scratch[14], 2 * C_N, &cnt));
-    unsigned long long* qlen = cnt + C_N;
     void* hp = nullptr;
     GIR_TRY(pinned(g, 256, &hp));
     unsigned long long* hc = static_cast<unsigned long long*>(hp);
@@ -287,19 +339,31 @@ int bct_build(gir_dev* g) {
     };
     // 1. BFS forest; order[] holds the levels back to back, lvl_off their boundaries
     GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 2 * C_N, g->stream));
-    k_roots<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, scc, parent, depth, order, cnt);
+    uint8_t* nontrivial = nullptr;
+    int32_t* hdeg = nullptr;
+    GIR_TRY(ensure_n(g, g->work[6], V + 1, &nontrivial));
+    GIR_TRY(ensure_n(g, g->work[7], V + 1, &hdeg));
+    GIR_CUDA(g, cudaMemsetAsync(nontrivial, 0, V, g->stream));
+    k_mark_nontrivial<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, scc, nontrivial);
+    GIR_LAUNCH(g, "k_mark_nontrivial");
+    k_h_deg<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, scc, nontrivial, g->sym.deg, hdeg);
+    GIR_LAUNCH(g, "k_h_deg");
+    h.sym.deg = hdeg;
+    k_roots<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, scc, nontrivial, parent, depth, order, cnt);
     GIR_LAUNCH(g, "k_roots");
     GIR_TRY(read());
     std::vector<int64_t> lvl_off{0, (int64_t)hc[C_Q]};
     for (int32_t L = 0;; ++L) {
         const int64_t lo = lvl_off[L], n = lvl_off[L + 1] - lo;
         if (n == 0) break;
-        const unsigned long long nn = (unsigned long long)n;
-        GIR_CUDA(g, cudaMemcpyAsync(qlen, &nn, sizeof(nn), cudaMemcpyHostToDevice, g->stream));
         GIR_CUDA(g, cudaMemsetAsync(&cnt[C_Q], 0, sizeof(unsigned long long), g->stream));
-        k_forest_level<<<grid_for(g, n * 32, kBlock), kBlock, 0, g->stream>>>(order + lo, qlen, h, parent, depth, L,
-                                                                             order + lo + n, cnt);
-        GIR_LAUNCH(g, "k_forest_level");
+        // (`scan` serves as the level's row-length prefix here; the preorder step reuses it later)
+        k_level_deg<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(order + lo, n, h.sym.deg, scan);
+        GIR_LAUNCH(g, "k_level_deg");
+        GIR_TRY(exclusive_scan_i64(g, scan, scan, n + 1));
+        k_forest_balanced<<<g->num_sms * 8, kBlock, 0, g->stream>>>(order + lo, n, scan, h, parent, depth, L,
+                                                                    order + lo + n, cnt);
+        GIR_LAUNCH(g, "k_forest_balanced");
         GIR_TRY(read());
         lvl_off.push_back(lvl_off.back() + (int64_t)hc[C_Q]);
     }
@@ -341,7 +405,11 @@ int bct_build(gir_dev* g) {
     GIR_CUDA(g, cudaMemcpyAsync(high, pre, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, g->stream));
     k_uf_init<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(uf, V);
     GIR_LAUNCH(g, "k_uf_init");
-    k_nontree<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, h, parent, pre, nd, low, high, uf, &cnt[C_ERR]);
+    int4* vinfo = nullptr;
+    GIR_TRY(ensure_n(g, g->work[5], V + 1, &vinfo));
+    k_pack_vinfo<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, pre, nd, parent, scc, vinfo);
+    GIR_LAUNCH(g, "k_pack_vinfo");
+    k_nontree<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, h, vinfo, low, high, uf, &cnt[C_ERR]);
     GIR_LAUNCH(g, "k_nontree");
     for (int L = D - 1; L >= 1; --L) {
         const int64_t n = lvl_off[L + 1] - lvl_off[L];

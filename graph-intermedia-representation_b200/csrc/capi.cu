@@ -2,6 +2,7 @@
 // update pipeline, getters and query entry points.
 #include <sys/stat.h>
 
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -137,10 +138,6 @@ __global__ void k_dag_split(const uint64_t* keys, int64_t n, int32_t* src, int32
     }
 }
 
-__global__ void k_gather_set_ranks(const int32_t* scc, const int32_t* rank_of_label, int64_t V, int32_t* out) {
-    GRID_STRIDE(v, V) out[v] = rank_of_label[scc[v]];
-}
-
 // Where a call writes an output: the caller's device buffer, or the handle's staging buffer
 // that is copied to the caller's host buffer afterwards.
 int out_target(gir_dev* g, void* user, size_t bytes, DevBuf& stage, void** dev) {
@@ -273,10 +270,20 @@ int invalidate_after_update(gir_dev* g) {
     return GIR_OK;
 }
 
+// Brings every built layer up to date, timing each (phases 1..3 of gir_dev_batch_times).
 int rebuild_layers(gir_dev* g) {
+    double t = now_ms();
     if (g->wcc_built) GIR_TRY(wcc_build(g));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    g->b_ms[1] = now_ms() - t;
+    t = now_ms();
     if (g->scc_built) GIR_TRY(scc_build(g));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    g->b_ms[2] = now_ms() - t;
+    t = now_ms();
     if (g->bct_built) GIR_TRY(bct_build(g));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    g->b_ms[3] = now_ms() - t;
     return GIR_OK;
 }
 
@@ -286,6 +293,8 @@ int rebuild_layers(gir_dev* g) {
 int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n) {
     const int64_t V = g->V;
     g->b_ins = g->b_del = g->b_noop = g->b_invalid = 0;
+    for (double& x : g->b_ms) x = 0;
+    const double t_start = now_ms();
     if (n <= 0) return GIR_OK;
     const void *du, *dv, *dins;
     DevBuf su, sv, si;
@@ -386,8 +395,9 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     GIR_TRY(store_apply_ops(g, g->sym, sym_ins, nsi, sym_del, nsd, false));
 
     GIR_TRY(invalidate_after_update(g));
-    GIR_TRY(rebuild_layers(g));
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    g->b_ms[0] = now_ms() - t_start;
+    GIR_TRY(rebuild_layers(g));
     return GIR_OK;
 }
 
@@ -445,6 +455,18 @@ int query_sets(gir_dev* g, const int64_t* set_beg_user, const int32_t* srcs, int
 }
 
 }  // namespace
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void trace_mark(gir_dev* g, const char* what) {
+    if (!g->trace_on) return;
+    cudaStreamSynchronize(g->stream);
+    const double t = now_ms();
+    std::fprintf(stderr, "[gir] %-28s %9.3f ms\n", what, g->trace_t > 0 ? t - g->trace_t : 0.0);
+    g->trace_t = t;
+}
 
 void set_thread_error(const std::string& msg) { g_create_err = msg; }
 
@@ -676,6 +698,12 @@ int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t h
     g->wrule_seed = seed;
     g->wrule_lo = lo;
     g->wrule_hi = hi;
+    return GIR_OK;
+}
+
+int gir_dev_batch_times(gir_dev_t* g, double* ms4) {
+    if (!g || !ms4) return GIR_ERR_INVALID;
+    for (int i = 0; i < 4; ++i) ms4[i] = g->b_ms[i];
     return GIR_OK;
 }
 

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -119,6 +120,7 @@ struct gir_dev {
 
     // Batch statistics
     int64_t b_ins = 0, b_del = 0, b_noop = 0, b_invalid = 0;
+    double b_ms[4] = {0, 0, 0, 0};    // phases of the last batch: store, WCC, SCC, BCT
 
     // Schedule
     int schedule = GIR_SCHEDULE_FIXED;
@@ -134,6 +136,10 @@ struct gir_dev {
     std::vector<int32_t> trace_y;     // the class taken for each row
     double wstat[2][2] = {{0, 0}, {0, 0}};  // per weight mode: mean and max weight (set with ws)
     std::string err;
+    // Phase trace on stderr (environment GIR_TRACE=1): each mark synchronizes and prints the
+    // wall time since the previous one, and every scratch allocation is reported.
+    bool trace_on = std::getenv("GIR_TRACE") != nullptr;
+    double trace_t = 0;
 };
 
 namespace gir {
@@ -146,6 +152,11 @@ void set_thread_error(const std::string& msg);
 int cuda_check(gir_dev* g, cudaError_t e, const char* what);
 #define GIR_CUDA(g, call) GIR_TRY(::gir::cuda_check((g), (call), #call))
 #define GIR_LAUNCH(g, what) GIR_TRY(::gir::cuda_check((g), cudaGetLastError(), what))
+
+// Monotonic wall clock in ms.
+double now_ms();
+// With tracing on: synchronizes the handle's stream, prints `what` and the ms since the last mark.
+void trace_mark(gir_dev* g, const char* what);
 
 // Grows a device buffer to at least `bytes` (contents not kept).
 int ensure(gir_dev* g, DevBuf& b, size_t bytes);

@@ -22,10 +22,12 @@ int cuda_check(gir_dev* g, cudaError_t e, const char* what) {
 
 int ensure(gir_dev* g, DevBuf& b, size_t bytes) {
     if (b.bytes >= bytes && b.p) return GIR_OK;
+    const double t0 = g->trace_on ? now_ms() : 0.0;
     if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
     size_t want = bytes < 256 ? 256 : bytes;
     want = (want + 255) & ~(size_t)255;
     cudaError_t e = cudaMalloc(&b.p, want);
+    if (g->trace_on) std::fprintf(stderr, "[gir] alloc %zu bytes: %.3f ms\n", want, now_ms() - t0);
     if (e != cudaSuccess) {
         b.p = nullptr;
         cudaGetLastError();

@@ -99,25 +99,52 @@ __global__ void k_pivot(int64_t V, const int32_t* label, const int32_t* indeg, c
     }
 }
 
-// Reach over unassigned vertices whose mark is not `epoch` yet (marks them).
-__global__ void __launch_bounds__(kBlock) k_reach(const int32_t* q, const unsigned long long* qlen, CSRView c,
-                                                  const int32_t* label, int32_t* mark, int32_t epoch, int32_t* nq,
-                                                  unsigned long long* cnt) {
-    warp_expand(q, (int64_t)*qlen, c, nq, &cnt[C_Q], [&](int32_t, int32_t w) {
-        if (label[w] != -1 || mark[w] == epoch) return false;
-        return atomicExch(&mark[w], epoch) != epoch;
-    });
+// Edge-balanced reach (the pivot's forward / backward search): the frontier's rows are cut into
+// equal chunks after a scan of their lengths, so hubs do not serialize a warp.
+//   forward:  w joins when unassigned and not yet marked `epoch` (it gets the mark);
+//   backward: w joins when marked `epoch` by the forward search and still unassigned (it gets
+//             the pivot's label: FW ∩ BW = SCC(pivot)).
+__global__ void k_frontier_deg(const int32_t* q, int64_t n, const int32_t* deg, int64_t* pref) {
+    GRID_STRIDE(i, n) pref[i] = deg[q[i]];
+    if (blockIdx.x == 0 && threadIdx.x == 0) pref[n] = 0;
 }
 
-// Backward reach from the pivot over unassigned vertices that the forward reach marked:
-// they form SCC(pivot) and get its label.
-__global__ void __launch_bounds__(kBlock) k_reach_bw_in_fw(const int32_t* q, const unsigned long long* qlen, CSRView bw,
-                                                           int32_t* label, const int32_t* mark, int32_t epoch,
-                                                           int32_t pivot, int32_t* nq, unsigned long long* cnt) {
-    warp_expand(q, (int64_t)*qlen, bw, nq, &cnt[C_Q], [&](int32_t, int32_t w) {
-        if (mark[w] != epoch) return false;
-        return atomicCAS(&label[w], -1, pivot) == -1;
-    });
+constexpr int kReachChunk = 32 * 16;
+
+template <bool Backward>
+__global__ void __launch_bounds__(kBlock) k_reach_balanced(const int32_t* q, int64_t nq, const int64_t* pref, CSRView c,
+                                                           int32_t* label, int32_t* mark, int32_t epoch, int32_t pivot,
+                                                           int32_t* out, unsigned long long* cnt) {
+    const int64_t total = pref[nq];
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c0 = warp * kReachChunk; c0 < total; c0 += nwarps * kReachChunk) {
+        const int64_t c1 = c0 + kReachChunk < total ? c0 + kReachChunk : total;
+        const int64_t key = c0 + lane < total ? c0 + lane : total - 1;
+        int64_t lo = 0, hi = nq - 1;
+        while (lo < hi) {
+            const int64_t m = (lo + hi + 1) >> 1;
+            if (pref[m] <= key) lo = m; else hi = m - 1;
+        }
+        int64_t i = lo;
+        for (int64_t base = c0; base < c1; base += 32) {
+            const int64_t p = base + lane;
+            bool push = false;
+            int32_t w = 0;
+            if (p < c1) {
+                while (pref[i + 1] <= p) ++i;
+                const int32_t u = q[i];
+                w = c.adj[c.beg[u] + (p - pref[i])];
+                if (!Backward) {
+                    if (label[w] == -1 && mark[w] != epoch) push = atomicExch(&mark[w], epoch) != epoch;
+                } else {
+                    if (mark[w] == epoch && label[w] == -1) push = atomicCAS(&label[w], -1, pivot) == -1;
+                }
+            }
+            warp_append(push, w, out, &cnt[C_Q]);
+        }
+    }
 }
 
 // Colour propagation: colour(w) = max(colour(w), colour(u)) along forward edges between
@@ -198,48 +225,24 @@ __global__ void __launch_bounds__(kBlock) k_cross_keys(int64_t V, CSRView fw, co
     });
 }
 
-__global__ void k_dag_dst(const uint64_t* keys, int64_t n, int32_t* dst) {
-    GRID_STRIDE(i, n) dst[i] = (int32_t)(keys[i] & 0xffffffffULL);
-}
-
 __global__ void k_distinct_u64(const uint64_t* keys, int64_t n, uint8_t* flag) {
     GRID_STRIDE(i, n) flag[i] = (i == 0 || keys[i] != keys[i - 1]);
 }
 
-// ---- topological levels over the condensation DAG (rows: keys sorted by source label) ----
-__global__ void k_dag_indeg(const uint64_t* keys, int64_t n, int32_t* indeg) {
-    GRID_STRIDE(i, n) atomicAdd(&indeg[(int64_t)(keys[i] & 0xffffffffULL)], 1);
-}
-
-__global__ void k_dag_rows(const uint64_t* keys, int64_t n, int64_t* first, int32_t* cnt) {
+// One round of longest-path levels over the condensation edges: level(b) >= level(a) + 1 for
+// every edge a -> b. Edge-parallel with a plain pre-check, so only raises take an atomic (no
+// hot counter: a node with many in-edges, like the giant SCC, is raised a few times, not
+// decremented once per edge as in Kahn's algorithm).
+__global__ void k_dag_level_round(const uint64_t* keys, int64_t n, int32_t* level, unsigned long long* changed) {
+    unsigned long long c = 0;
     GRID_STRIDE(i, n) {
-        const int64_t a = (int64_t)(keys[i] >> 32);
-        if (i == 0 || (int64_t)(keys[i - 1] >> 32) != a) first[a] = i;
-        atomicAdd(&cnt[a], 1);
+        const uint64_t k = keys[i];
+        const int32_t a = (int32_t)(k >> 32), b = (int32_t)(k & 0xffffffffULL);
+        const int32_t cand = level[a] + 1;
+        if (cand > level[b] && atomicMax(&level[b], cand) < cand) ++c;
     }
-}
-
-__global__ void k_dag_sources(int64_t V, const int32_t* label, const int32_t* indeg, int32_t* level, int32_t* q,
-                              unsigned long long* cnt) {
-    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t v = base + threadIdx.x;
-        bool src = false;
-        if (v < V && label[v] == (int32_t)v) {
-            if (indeg[v] == 0) { src = true; level[v] = 0; }
-        }
-        warp_append(src, (int32_t)v, q, &cnt[C_Q]);
-    }
-}
-
-// One Kahn round: DAG nodes of the queue release their out-edges (rows: first / rcnt / dst).
-__global__ void __launch_bounds__(kBlock) k_dag_step(const int32_t* q, const unsigned long long* qlen, CSRView dagc,
-                                                     int32_t* indeg, int32_t* level, int32_t L, int32_t* nq,
-                                                     unsigned long long* cnt) {
-    warp_expand(q, (int64_t)*qlen, dagc, nq, &cnt[C_Q], [&](int32_t, int32_t b) {
-        if (atomicSub(&indeg[b], 1) != 1) return false;
-        level[b] = L + 1;
-        return true;
-    });
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane_id() == 0 && c) atomicAdd(changed, c);
 }
 
 __global__ void k_rank_keys(int64_t V, const int32_t* label, const int32_t* level, uint64_t* keys,
@@ -306,6 +309,7 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
         return GIR_OK;
     };
 
+    trace_mark(g, "scc: start");
     // 1. trim-1
     GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 2 * C_N, g->stream));
     k_trim_init<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, fw, bw, label, indeg, outdeg, qa, cnt);
@@ -321,6 +325,7 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
         return GIR_OK;
     }));
 
+    trace_mark(g, "scc: trim");
     // 2. forward-backward from the max-degree pivot
     GIR_CUDA(g, cudaMemsetAsync(mark, 0, sizeof(int32_t) * V, g->stream));
     GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
@@ -337,23 +342,34 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
         const unsigned long long one = 1;
         GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
         GIR_CUDA(g, cudaMemcpyAsync(&cnt[C_Q], &one, sizeof(one), cudaMemcpyHostToDevice, g->stream));
-        GIR_TRY(run_queue(qa, qb, 1, [&](int32_t* in, int32_t* out, int64_t m) -> int {
-            k_reach<<<blocks_for_queue(m), kBlock, 0, g->stream>>>(in, qlen, fw, label, mark, epoch, out, cnt);
-            GIR_LAUNCH(g, "k_reach");
+        int64_t* pref = nullptr;
+        GIR_TRY(ensure_n(g, g->scratch[7], V + 2, &pref));
+        // level-synchronous, edge-balanced: frontier degrees, scan, chunked expansion
+        auto balanced = [&](const CSRView& c, bool backward) -> int {
+            int64_t n = 1;
+            while (n > 0) {
+                k_frontier_deg<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(qa, n, c.deg, pref);
+                GIR_LAUNCH(g, "k_frontier_deg");
+                GIR_TRY(exclusive_scan_i64(g, pref, pref, n + 1));
+                GIR_CUDA(g, cudaMemsetAsync(&cnt[C_Q], 0, sizeof(unsigned long long), g->stream));
+                if (backward)
+                    k_reach_balanced<true><<<grid, kBlock, 0, g->stream>>>(qa, n, pref, c, label, mark, epoch, pivot, qb, cnt);
+                else
+                    k_reach_balanced<false><<<grid, kBlock, 0, g->stream>>>(qa, n, pref, c, label, mark, epoch, pivot, qb, cnt);
+                GIR_LAUNCH(g, "k_reach_balanced");
+                std::swap(qa, qb);
+                GIR_TRY(lp.read(&n));
+            }
             return GIR_OK;
-        }));
+        };
+        GIR_TRY(balanced(fw, false));
         // backward reach inside the forward set: SCC(pivot)
         GIR_CUDA(g, cudaMemcpyAsync(label + pivot, &pivot, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
         GIR_CUDA(g, cudaMemcpyAsync(qa, &pivot, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
-        GIR_CUDA(g, cudaMemcpyAsync(&cnt[C_Q], &one, sizeof(one), cudaMemcpyHostToDevice, g->stream));
-        GIR_TRY(run_queue(qa, qb, 1, [&](int32_t* in, int32_t* out, int64_t m) -> int {
-            k_reach_bw_in_fw<<<blocks_for_queue(m), kBlock, 0, g->stream>>>(in, qlen, bw, label, mark, epoch, pivot,
-                                                                            out, cnt);
-            GIR_LAUNCH(g, "k_reach_bw_in_fw");
-            return GIR_OK;
-        }));
+        GIR_TRY(balanced(bw, true));
     }
 
+    trace_mark(g, "scc: fw-bw");
     // 3. colour propagation rounds until every vertex is assigned
     int32_t* inq = mark;
     int32_t round = 1;
@@ -381,6 +397,8 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
         }));
     }
 
+    if (g->trace_on) std::fprintf(stderr, "[gir] scc: colour rounds %d\n", (int)round);
+    trace_mark(g, "scc: colour");
     // 4. canonical labels
     int32_t* mn = color;
     k_fill<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(mn, V, INT32_MAX);
@@ -399,6 +417,7 @@ int scc_build(gir_dev* g) {
     int32_t* label = nullptr;
     GIR_TRY(ensure_n(g, g->scc, V + 1, &label));
     GIR_TRY(scc_labels(g, label, &g->n_scc));
+    trace_mark(g, "scc: labels");
 
     // condensation edges: cross keys, radix sort, unique
     const int64_t cap = g->fw.cap;
@@ -430,53 +449,24 @@ int scc_build(gir_dev* g) {
         GIR_TRY(select_flagged_u64(g, keys, flag, dag, n_cross, &n_dag));
     }
     g->n_dag = n_dag;
+    trace_mark(g, "scc: dag edges");
 
-    // topological ranks by Kahn levels
-    int32_t *indeg = nullptr, *level = nullptr, *qa = nullptr, *qb = nullptr, *rcnt = nullptr, *rank_of = nullptr;
-    int64_t* first = nullptr;
-    int32_t *rank = nullptr, *dst = nullptr;
-    GIR_TRY(ensure_n(g, g->scratch[11], n_dag + 1, &dst));
-    GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &indeg));
+    // topological ranks: longest-path levels over the condensation edges, rounds until stable
+    // (at most the DAG's depth + 1 rounds)
+    int32_t *level = nullptr, *rank_of = nullptr, *rank = nullptr;
     GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &level));
-    GIR_TRY(ensure_n(g, g->scratch[2], V + 1, &qa));
-    GIR_TRY(ensure_n(g, g->scratch[3], V + 1, &qb));
-    GIR_TRY(ensure_n(g, g->scratch[4], V + 1, &rcnt));
     GIR_TRY(ensure_n(g, g->scratch[5], V + 1, &rank_of));
-    GIR_TRY(ensure_n(g, g->scratch[10], V + 1, &first));
     GIR_TRY(ensure_n(g, g->scc_rank, V + 1, &rank));
-    GIR_CUDA(g, cudaMemsetAsync(indeg, 0, sizeof(int32_t) * V, g->stream));
-    GIR_CUDA(g, cudaMemsetAsync(rcnt, 0, sizeof(int32_t) * V, g->stream));
     GIR_CUDA(g, cudaMemsetAsync(level, 0, sizeof(int32_t) * V, g->stream));
-    if (n_dag > 0) {
-        k_dag_indeg<<<grid_for(g, n_dag, kBlock), kBlock, 0, g->stream>>>(dag, n_dag, indeg);
-        GIR_LAUNCH(g, "k_dag_indeg");
-        k_dag_rows<<<grid_for(g, n_dag, kBlock), kBlock, 0, g->stream>>>(dag, n_dag, first, rcnt);
-        GIR_LAUNCH(g, "k_dag_rows");
-        k_dag_dst<<<grid_for(g, n_dag, kBlock), kBlock, 0, g->stream>>>(dag, n_dag, dst);
-        GIR_LAUNCH(g, "k_dag_dst");
-    }
-    const CSRView dagc{first, rcnt, dst, nullptr};
-    unsigned long long* qlen = cnt + C_N;
-    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
-    if (V > 0) {
-        k_dag_sources<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, indeg, level, qa, cnt);
-        GIR_LAUNCH(g, "k_dag_sources");
-    }
-    GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
-    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-    int64_t nq = (int64_t)hc[C_Q];
-    int32_t L = 0;
-    while (nq > 0) {
-        GIR_CUDA(g, cudaMemcpyAsync(qlen, &cnt[C_Q], sizeof(unsigned long long), cudaMemcpyDeviceToDevice, g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(&cnt[C_Q], 0, sizeof(unsigned long long), g->stream));
-        k_dag_step<<<grid_for(g, nq * 32, kBlock), kBlock, 0, g->stream>>>(qa, qlen, dagc, indeg, level, L, qb, cnt);
-        GIR_LAUNCH(g, "k_dag_step");
-        std::swap(qa, qb);
+    for (int64_t round = 0; n_dag > 0 && round <= V; ++round) {
+        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+        k_dag_level_round<<<grid_for(g, n_dag, kBlock), kBlock, 0, g->stream>>>(dag, n_dag, level, &cnt[C_Q]);
+        GIR_LAUNCH(g, "k_dag_level_round");
         GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
         GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-        nq = (int64_t)hc[C_Q];
-        ++L;
+        if (hc[C_Q] == 0) break;
     }
+    trace_mark(g, "scc: levels");
     // rank = position in (level, label) order
     GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
     if (V > 0) {
@@ -493,6 +483,7 @@ int scc_build(gir_dev* g) {
         k_rank_gather<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, rank_of, rank);
         GIR_LAUNCH(g, "k_rank_gather");
     }
+    trace_mark(g, "scc: ranks");
     g->scc_built = true;
     return GIR_OK;
 }

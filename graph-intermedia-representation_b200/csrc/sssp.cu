@@ -22,7 +22,6 @@ namespace gir {
 namespace {
 
 constexpr int kBlock = 256;
-constexpr int kWarps = kBlock / 32;
 constexpr uint64_t kInf = ~0ull;
 
 #define GRID_STRIDE(i, n) \

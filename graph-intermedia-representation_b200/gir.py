@@ -178,6 +178,12 @@ class DeviceGraph:
         self._ck(dev_lib().gir_dev_batch_stats(self._h, *[ctypes.byref(v) for v in vals]), "batch_stats")
         return dict(zip(("inserted", "deleted", "noop", "invalid"), (v.value for v in vals)))
 
+    def batch_times(self):
+        """Wall ms of the last batch's phases: store merge, WCC, SCC + DAG, blocks."""
+        out = np.zeros(4, np.float64)
+        self._ck(dev_lib().gir_dev_batch_times(self._h, ptr(out)), "batch_times")
+        return dict(zip(("store", "wcc", "scc", "bct"), out.tolist()))
+
     def set_weight_rule(self, seed, lo, hi):
         self._ck(dev_lib().gir_dev_set_weight_rule(self._h, seed, lo, hi), "set_weight_rule")
 

@@ -151,6 +151,10 @@ int gir_dev_sssp_sets(gir_dev_t* g, const int64_t* set_beg, const int32_t* set_s
  * lo, hi) set by gir_dev_set_weight_rule (default: the hash weight of GIR::edgeWeight). */
 int gir_dev_apply_batch(gir_dev_t* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n);
 
+/* Wall time (ms) of the phases of the last apply_batch: [0] normalisation and the merges into the
+ * edge store, [1] WCC, [2] SCC + DAG + ranks, [3] blocks. */
+int gir_dev_batch_times(gir_dev_t* g, double* ms4);
+
 /* Weight rule for edges inserted into a graph with stored weights (see apply_batch). */
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi);
 

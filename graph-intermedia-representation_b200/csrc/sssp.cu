@@ -122,7 +122,7 @@ struct Relax {
 
 // Work-balanced relaxation: k_relax_prep turns the queue into items (one per vertex with work),
 // an exclusive scan of the items' work (edges x lanes) numbers all (edge, lane) pairs, and
-// k_relax_tile processes them in equal tiles, so a hub with many lanes is spread over the grid.
+// k_relax processes them in equal runs, so a hub with many lanes is spread over the grid.
 struct Items {
     int32_t* u;
     int64_t* eb;
@@ -146,13 +146,15 @@ __global__ void k_light_split(int64_t V, const int64_t* wb, const int32_t* wdeg,
 
 // Takes every queued vertex's lanes (clearing them), does the settle bookkeeping and appends an
 // item (vertex, first edge, lane mask, work = edges x lanes) for every vertex with work; the
-// item count goes to cnt[S_ITEMS].
+// item count goes to cnt[S_ITEMS]. Item slots past the count keep the zero work they were
+// cleared to, so a scan over all n + 1 slots needs no count from the host.
 __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, const int32_t* nlight, Items it) {
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
         int32_t u = 0;
         unsigned long long m = 0;
         int64_t eb = 0, work = 0;
+        bool settles = false;
         if (i < n) {
             u = q[i];
             if (heavy) {
@@ -161,13 +163,14 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
             } else {
                 m = a.curmask[u];
                 a.curmask[u] = 0ull;
-                if (m && atomicOr(&a.setmask[u], m) == 0ull) a.setq[atomicAdd(&a.cnt[S_SET], 1ull)] = u;
+                settles = m && atomicOr(&a.setmask[u], m) == 0ull;
             }
             const int64_t b = a.wb[u];
             const int32_t nlu = nlight[u];
             eb = heavy ? b + nlu : b;
             work = (int64_t)(heavy ? a.wdeg[u] - nlu : nlu) * __popcll(m);
         }
+        warp_append(settles, u, a.setq, &a.cnt[S_SET]);
         const bool has = work > 0;
         const unsigned bal = __ballot_sync(0xffffffffu, has);
         if (bal) {
@@ -185,125 +188,121 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
     }
 }
 
-constexpr int kTileThreads = 256;
-constexpr int kPairs = 4;                          // pairs in flight per thread
-constexpr int kTile = kTileThreads * kPairs;       // (edge, lane) pairs per CTA tile
+constexpr int kRelaxThreads = 256;
+constexpr int kPairs = 2;  // pairs in flight per thread (with 6 CTAs per SM: measured best)
 
-// Load-balanced relaxation: CTA tiles of kTile consecutive pairs of the whole item list. The
-// items overlapping a tile (at most kTile, every item has work) are staged in shared memory;
-// each pair finds its item by binary search there, so no thread walks item boundaries through
-// global memory. Pairs are enumerated edge-major within an item: with many lanes active,
-// consecutive threads update consecutive lanes of one distance row.
-__global__ void __launch_bounds__(kTileThreads) k_relax_tile(const unsigned long long* n_items, Items it, Relax a) {
-    __shared__ int32_t s_off[kTile + 1];            // item start, relative to the tile start
-    __shared__ int64_t s_eb[kTile];
-    __shared__ unsigned long long s_m[kTile];
-    __shared__ int32_t s_u[kTile];
-    __shared__ int64_t s_range[2];
+// Largest e in [lo, hi] with pref[e] <= key, for a strictly increasing pref with
+// pref[lo] <= key. One warp, 32 probes a round: the window shrinks 32-fold per dependent load.
+__device__ __forceinline__ int64_t warp_search(const int64_t* pref, int64_t lo, int64_t hi, int64_t key) {
+    const int ln = lane_id();
+    while (hi > lo) {
+        const int64_t step = (hi - lo + 31) / 32;
+        const int64_t p = lo + (int64_t)(ln + 1) * step;
+        const bool c = p <= hi && pref[p] <= key;
+        const int t = __popc(__ballot_sync(0xffffffffu, c));
+        if (t > 0) lo += (int64_t)t * step;
+        hi = lo + step - 1 < hi ? lo + step - 1 : hi;
+    }
+    return lo;
+}
+
+// Load-balanced relaxation over all (edge, lane) pairs of the item list, numbered by the
+// exclusive scan of the items' work. Every warp takes one contiguous run of pairs and finds the
+// item holding its first pair with one warp search. It then walks windows of 32 consecutive
+// items, one item per lane in registers: a pair finds its item by a binary search over the
+// window through shuffles, so no shared memory and no block barrier is involved and warps
+// proceed independently. Pairs are enumerated edge-major within an item: with many lanes
+// active, consecutive threads update consecutive lanes of one distance row.
+__global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long long* n_items, Items it, Relax a) {
     const int64_t n = (int64_t)*n_items;
     if (n == 0) return;
     const int64_t total = it.pref[n];
-    for (int64_t t0 = (int64_t)blockIdx.x * kTile; t0 < total; t0 += (int64_t)gridDim.x * kTile) {
-        const int64_t t1 = t0 + kTile < total ? t0 + kTile : total;
-        if (threadIdx.x < 2) {  // items holding the tile's first and last pair
-            const int64_t key = threadIdx.x == 0 ? t0 : t1 - 1;
-            int64_t lo = 0, hi = n - 1;
-            while (lo < hi) {
-                const int64_t mid = (lo + hi + 1) >> 1;
-                if (it.pref[mid] <= key) lo = mid; else hi = mid - 1;
-            }
-            s_range[threadIdx.x] = lo;
+    const int ln = lane_id();
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t per = (((total + nw - 1) / nw) + 31) & ~(int64_t)31;
+    const int64_t c0 = gw * per;
+    const int64_t c1 = c0 + per < total ? c0 + per : total;
+    if (c0 >= c1) return;
+    int64_t e0 = warp_search(it.pref, 0, n - 1, c0);
+    int64_t p = c0;
+    while (p < c1) {
+        // window: items e0 .. e0+31, lane j holding item e0+j
+        const int64_t ej = e0 + ln;
+        int64_t pj = INT64_MAX, ebj = 0;
+        unsigned long long mj = 0;
+        int32_t uj = 0;
+        if (ej < n) {
+            pj = it.pref[ej];
+            ebj = it.eb[ej];
+            mj = it.m[ej];
+            uj = it.u[ej];
         }
-        __syncthreads();
-        const int64_t e0 = s_range[0];
-        const int ne = (int)(s_range[1] - e0 + 1);
-        for (int j = threadIdx.x; j < ne; j += kTileThreads) {
-            const int64_t e = e0 + j;
-            s_off[j] = (int32_t)(it.pref[e] - t0);  // (the first item may start before the tile)
-            s_eb[j] = it.eb[e];
-            s_m[j] = it.m[e];
-            s_u[j] = it.u[e];
-        }
-        if (threadIdx.x == 0) s_off[ne] = (int32_t)(it.pref[s_range[1] + 1] - t0);
-        __syncthreads();
-        int32_t w[kPairs], s[kPairs];
-        int64_t k[kPairs];
-        uint64_t du[kPairs];
-        bool on[kPairs];
+        const int64_t wnext = e0 + 32 < n ? it.pref[e0 + 32] : total;
+        const int64_t wend = wnext < c1 ? wnext : c1;
+        for (; p < wend; p += 32 * kPairs) {
+            int32_t w[kPairs], sl[kPairs];
+            int64_t k[kPairs];
+            uint64_t du[kPairs];
+            bool on[kPairs];
 #pragma unroll
-        for (int j = 0; j < kPairs; ++j) {
-            const int64_t p = t0 + j * kTileThreads + threadIdx.x;
-            on[j] = p < t1;
-            if (on[j]) {
-                const int32_t rel = (int32_t)(p - t0);
-                int lo = 0, hi = ne - 1;  // item: largest x with s_off[x] <= rel
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s_off[mid] <= rel) lo = mid; else hi = mid - 1;
+            for (int j = 0; j < kPairs; ++j) {
+                const int64_t q = p + j * 32 + ln;
+                on[j] = q < wend;
+                int x = 0;  // largest x with pref(x) <= q
+#pragma unroll
+                for (int b = 16; b; b >>= 1) {
+                    const int64_t v = __shfl_sync(0xffffffffu, pj, x + b);
+                    if (v <= q) x += b;
                 }
-                const unsigned long long m = s_m[lo];
-                const int pc = __popcll(m);
-                const int32_t q2 = rel - s_off[lo];
-                k[j] = s_eb[lo] + q2 / pc;
-                s[j] = nth_bit(m, q2 % pc);
-                du[j] = a.dist[(int64_t)s_u[lo] * a.nl + s[j]];
+                const int64_t px = __shfl_sync(0xffffffffu, pj, x);
+                const int64_t ebx = __shfl_sync(0xffffffffu, ebj, x);
+                const unsigned long long mx = __shfl_sync(0xffffffffu, mj, x);
+                const int32_t ux = __shfl_sync(0xffffffffu, uj, x);
+                if (on[j]) {
+                    const int pc = __popcll(mx);
+                    const int32_t q2 = (int32_t)(q - px);
+                    k[j] = ebx + q2 / pc;
+                    sl[j] = nth_bit(mx, q2 % pc);
+                    du[j] = a.dist[(int64_t)ux * a.nl + sl[j]];
+                }
             }
-        }
-        uint32_t wt[kPairs];
+            uint32_t wt[kPairs];
 #pragma unroll
-        for (int j = 0; j < kPairs; ++j) {
-            if (on[j]) { w[j] = a.wadj[k[j]]; wt[j] = a.ww[k[j]]; } else { w[j] = 0; wt[j] = 0; }
-        }
-        uint64_t cur[kPairs];
+            for (int j = 0; j < kPairs; ++j) {
+                if (on[j]) { w[j] = a.wadj[k[j]]; wt[j] = a.ww[k[j]]; } else { w[j] = 0; wt[j] = 0; }
+            }
+            uint64_t cur[kPairs];
 #pragma unroll
-        for (int j = 0; j < kPairs; ++j)
-            cur[j] = on[j] ? *(volatile uint64_t*)&a.dist[(int64_t)w[j] * a.nl + s[j]] : 0ull;
+            for (int j = 0; j < kPairs; ++j)
+                cur[j] = on[j] ? *(volatile uint64_t*)&a.dist[(int64_t)w[j] * a.nl + sl[j]] : 0ull;
 #pragma unroll
-        for (int j = 0; j < kPairs; ++j) {
-            bool to_near = false, to_far = false;
-            if (on[j]) {
-                const uint64_t nd = du[j] + (uint64_t)wt[j];
-                if (nd < cur[j]) {  // plain pre-check: most relaxations lose
-                    const unsigned long long old =
-                        atomicMin((unsigned long long*)&a.dist[(int64_t)w[j] * a.nl + s[j]], (unsigned long long)nd);
-                    if (nd < old) {
-                        const unsigned long long bit = 1ull << s[j];
-                        if (nd < a.kend) to_near = atomicOr(&a.nextmask[w[j]], bit) == 0ull;
-                        else to_far = atomicOr(&a.farmask[w[j]], bit) == 0ull;
+            for (int j = 0; j < kPairs; ++j) {
+                bool to_near = false, to_far = false;
+                if (on[j]) {
+                    const uint64_t nd = du[j] + (uint64_t)wt[j];
+                    if (nd < cur[j]) {  // plain pre-check: most relaxations lose
+                        const unsigned long long old = atomicMin(
+                            (unsigned long long*)&a.dist[(int64_t)w[j] * a.nl + sl[j]], (unsigned long long)nd);
+                        if (nd < old) {
+                            const unsigned long long bit = 1ull << sl[j];
+                            if (nd < a.kend) to_near = atomicOr(&a.nextmask[w[j]], bit) == 0ull;
+                            else to_far = atomicOr(&a.farmask[w[j]], bit) == 0ull;
+                        }
                     }
                 }
+                warp_append(to_near, w[j], a.nextq, &a.cnt[S_NEAR]);
+                warp_append(to_far, w[j], a.farq, &a.cnt[S_FAR]);
             }
-            warp_append(to_near, w[j], a.nextq, &a.cnt[S_NEAR]);
-            warp_append(to_far, w[j], a.farq, &a.cnt[S_FAR]);
         }
-        __syncthreads();  // (the next tile overwrites the staged items)
+        p = wend;  // (the pairs of this window end exactly where item e0+32 begins)
+        e0 += 32;
     }
 }
 
-// Smallest live far distance (dist >= kend; smaller ones are settled already).
-__global__ void k_far_min(const int32_t* farq, const unsigned long long* nfar, const unsigned long long* farmask,
-                          const uint64_t* dist, int nl, uint64_t kend, unsigned long long* cnt) {
-    unsigned long long mn = kInf;
-    const int64_t n = (int64_t)*nfar;
-    GRID_STRIDE(i, n) {
-        const int32_t w = farq[i];
-        unsigned long long m = farmask[w];
-        while (m) {
-            const int s = __ffsll((long long)m) - 1;
-            m &= m - 1;
-            const uint64_t d = dist[(int64_t)w * nl + s];
-            if (d >= kend && d < mn) mn = d;
-        }
-    }
-    for (int o = 16; o; o >>= 1) {
-        const unsigned long long t = __shfl_xor_sync(0xffffffffu, mn, o);
-        mn = t < mn ? t : mn;
-    }
-    if (lane_id() == 0 && mn != kInf) atomicMin(&cnt[S_MIN], mn);
-}
-
-// Splits the far entries at the new bucket [lo, hi): lanes inside it become near work, later
-// lanes stay far (queued in farq2), settled lanes are dropped.
+// Splits the far entries at the bucket [lo, hi): lanes inside it become near work, later lanes
+// stay far (queued in farq2) and their smallest distance goes to cnt[S_MIN] (the bucket to jump
+// to when this one turns out empty); settled lanes are dropped.
 __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar, unsigned long long* farmask,
                             const uint64_t* dist, int nl, uint64_t lo, uint64_t hi, unsigned long long* nearmask,
                             int32_t* nearq, int32_t* farq2, unsigned long long* cnt) {
@@ -312,6 +311,7 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
         const int64_t i = base + threadIdx.x;
         bool to_near = false, to_far = false;
         int32_t w = 0;
+        unsigned long long mn = kInf;
         if (i < n) {
             w = farq[i];
             unsigned long long m = farmask[w], nm = 0, keep = 0;
@@ -319,8 +319,12 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
                 const int s = __ffsll((long long)m) - 1;
                 m &= m - 1;
                 const uint64_t d = dist[(int64_t)w * nl + s];
-                if (d >= lo && d < hi) nm |= 1ull << s;
-                else if (d >= hi) keep |= 1ull << s;
+                if (d >= lo && d < hi) {
+                    nm |= 1ull << s;
+                } else if (d >= hi) {
+                    keep |= 1ull << s;
+                    mn = d < mn ? d : mn;
+                }
             }
             farmask[w] = keep;
             to_far = keep != 0;
@@ -328,6 +332,11 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
         }
         warp_append(to_near, w, nearq, &cnt[S_NEAR]);
         warp_append(to_far, w, farq2, &cnt[S_FAR2]);
+        for (int o = 16; o; o >>= 1) {
+            const unsigned long long t = __shfl_xor_sync(0xffffffffu, mn, o);
+            mn = t < mn ? t : mn;
+        }
+        if (lane_id() == 0 && mn != kInf) atomicMin(&cnt[S_MIN], mn);
     }
 }
 
@@ -459,8 +468,10 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
     };
     const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
     MainTimer timer{g, g->params[GIR_PARAM_PROFILE] != 0.0};
-    // the relaxation is latency-bound: a full SM's worth of warps (8 CTAs x 256 threads) hides it
-    const int run_grid = g->num_sms * 8;
+    // the relaxation kernel gives every warp one contiguous run of pairs: one CTA per resident slot
+    int per_sm = 0;
+    GIR_CUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_relax, kRelaxThreads, 0));
+    const int run_grid = g->num_sms * (per_sm > 0 ? per_sm : 1);
     int32_t* nlight = nullptr;
     GIR_TRY(ensure_n(g, g->scratch[9], V + 1, &nlight));
     Items items;
@@ -507,25 +518,29 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         a.wb = ws.beg; a.wdeg = ws.deg; a.wadj = ws.adj; a.ww = ws.w; a.delta = D; a.nl = nl; a.dist = dist;
         a.farmask = farmask; a.setmask = setmask; a.setq = setq; a.cnt = cnt;
         uint64_t k = 0;
+        int64_t trace_pairs = 0, trace_passes = 0;
         // one relaxation pass over queue q (n entries): prep, scan of the work, balanced run
         k_light_split<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, ws.beg, ws.deg, ws.w, D, nlight);
         GIR_LAUNCH(g, "k_light_split");
         auto relax = [&](const int32_t* q, int64_t n, int heavy) -> int {
             GIR_CUDA(g, cudaMemsetAsync(cnt + S_ITEMS, 0, sizeof(unsigned long long), g->stream));
+            GIR_CUDA(g, cudaMemsetAsync(items.pref, 0, sizeof(int64_t) * (n + 1), g->stream));
             k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, nlight, items);
             GIR_LAUNCH(g, "k_relax_prep");
-            GIR_TRY(read());
-            const int64_t ni = (int64_t)hc[S_ITEMS];
-            st.launches++;
-            if (ni == 0) return GIR_OK;
-            GIR_CUDA(g, cudaMemsetAsync(items.pref + ni, 0, sizeof(int64_t), g->stream));
-            GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, ni + 1));
+            GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));
+            if (g->trace_on) {
+                int64_t tot = 0;
+                GIR_CUDA(g, cudaMemcpyAsync(&tot, items.pref + n, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
+                GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+                trace_pairs += tot;
+                ++trace_passes;
+            }
             GIR_TRY(timer.run([&]() -> int {
-                k_relax_tile<<<run_grid, kTileThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
-                GIR_LAUNCH(g, "k_relax_tile");
+                k_relax<<<run_grid, kRelaxThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
+                GIR_LAUNCH(g, "k_relax");
                 return GIR_OK;
             }));
-            st.launches += 3;  // the scan's two kernels, the tile kernel
+            st.launches += 4;  // prep, the scan's two kernels, the relaxation
             return GIR_OK;
         };
         while (true) {
@@ -548,29 +563,39 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
                 a.curmask = curmask; a.nextmask = nextmask; a.nextq = nextq; a.farq = farq;
                 GIR_TRY(relax(setq, n_set, 1));
             }
-            // next bucket: the smallest live far distance
-            GIR_CUDA(g, cudaMemsetAsync(cnt + S_MIN, 0xff, sizeof(unsigned long long), g->stream));
+            // next bucket: split the far entries at bucket k + 1; when that one is empty, jump to
+            // the bucket of the smallest distance still far
             GIR_TRY(read());
             n_far = (int64_t)hc[S_FAR];
             if (n_far == 0) break;
-            k_far_min<<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(farq, cnt + S_FAR, farmask, dist, nl, a.kend,
-                                                                            cnt);
-            GIR_LAUNCH(g, "k_far_min");
-            GIR_TRY(read());
-            const uint64_t mind = hc[S_MIN];
-            if (mind == kInf) break;  // only settled entries left
-            k = mind / D;
-            GIR_CUDA(g, cudaMemsetAsync(cnt + S_FAR2, 0, sizeof(unsigned long long), g->stream));
-            k_far_split<<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(farq, cnt + S_FAR, farmask, dist, nl, k * D,
-                                                                              (k + 1) * D, curmask, nearq, farq2, cnt);
-            GIR_LAUNCH(g, "k_far_split");
-            st.launches += 2;
-            std::swap(farq, farq2);
-            GIR_CUDA(g, cudaMemcpyAsync(cnt + S_FAR, cnt + S_FAR2, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
-                                        g->stream));
-            GIR_TRY(read());
-            n_near = (int64_t)hc[S_NEAR];
+            uint64_t lo = a.kend;
+            bool finished = false;
+            while (true) {
+                k = lo / D;
+                GIR_CUDA(g, cudaMemsetAsync(cnt + S_MIN, 0xff, sizeof(unsigned long long), g->stream));
+                GIR_CUDA(g, cudaMemsetAsync(cnt + S_FAR2, 0, sizeof(unsigned long long), g->stream));
+                k_far_split<<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(
+                    farq, cnt + S_FAR, farmask, dist, nl, k * D, (k + 1) * D, curmask, nearq, farq2, cnt);
+                GIR_LAUNCH(g, "k_far_split");
+                st.launches++;
+                std::swap(farq, farq2);
+                GIR_CUDA(g, cudaMemcpyAsync(cnt + S_FAR, cnt + S_FAR2, sizeof(unsigned long long),
+                                            cudaMemcpyDeviceToDevice, g->stream));
+                GIR_TRY(read());
+                n_near = (int64_t)hc[S_NEAR];
+                n_far = (int64_t)hc[S_FAR];
+                if (n_near > 0) break;
+                if (hc[S_MIN] == kInf) {  // nothing live is left far
+                    finished = true;
+                    break;
+                }
+                lo = hc[S_MIN];
+            }
+            if (finished) break;
         }
+        if (g->trace_on)
+            std::fprintf(stderr, "[gir] sssp group of %d lanes, delta %llu: %lld passes, %lld (edge, lane) pairs\n", nl,
+                         (unsigned long long)D, (long long)trace_passes, (long long)trace_pairs);
         k_sssp_reached<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(dist, V, nl, g->fw.deg, cnt);
         GIR_LAUNCH(g, "k_sssp_reached");
         if (nl > 1) {

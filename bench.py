@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--workload", default="rmat_lj", choices=["rmat_lj", "rmat_s20", "rmat_s16"])
     p.add_argument("--no-updates", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-schedule", action="store_true", help="skip the learned-vs-fixed schedule comparison")
     p.add_argument("--only", choices=["bfs", "sssp", "build"], default=None,
                    help="profiling runs: one call of one query kind (or the three layer builds and one "
                         "10K update batch), no timing and no JSON line")
@@ -233,6 +234,48 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def ev_time(stream, fn):
+    """Device ms of fn() between CUDA events on the handle's stream."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def compare_schedules(pkg, d, stream, sb, ss, lv, ds, weights, delta_fixed, reps):
+    """The same BFS and SSSP sources under the fixed heuristics (the reference's alpha/beta switch
+    and delta) and under the trained schedule network; results must be identical."""
+    import torch
+    native = pkg.native
+    out = {}
+    lv2, ds2 = torch.empty_like(lv), torch.empty_like(ds)
+    d.set_schedule(native.SCHEDULE_FIXED)
+    d.bfs(sb, out=lv)
+    d.sssp(ss[:1], delta=2048, weights=weights, out=ds[:1])  # (builds the weight-sorted rows)
+    t_bf = min(ev_time(stream, lambda: d.bfs(sb, out=lv)) for _ in range(reps))
+    t_sf = min(ev_time(stream, lambda: d.sssp(ss, delta=delta_fixed, weights=weights, out=ds)) for _ in range(reps))
+    d.use_learned_schedule()
+    d.bfs(sb, out=lv2)
+    t_bl = min(ev_time(stream, lambda: d.bfs(sb, out=lv2)) for _ in range(reps))
+    _, y_bfs = d.sched_trace()
+    t_sl = min(ev_time(stream, lambda: d.sssp(ss, delta=0, weights=weights, out=ds2)) for _ in range(reps))
+    _, y_sssp = d.sched_trace()
+    d.set_schedule(native.SCHEDULE_FIXED)
+    choices = pkg.DeviceGraph.delta_choices()
+    out["bfs"] = {"fixed_ms": t_bf, "learned_ms": t_bl, "speedup": t_bf / t_bl, "identical": bool(torch.equal(lv, lv2)),
+                  "learned_bottom_up_levels": int((y_bfs == 1).sum()), "levels": int(len(y_bfs))}
+    out["sssp"] = {"fixed_ms": t_sf, "learned_ms": t_sl, "speedup": t_sf / t_sl, "identical": bool(torch.equal(ds, ds2)),
+                   "fixed_delta": delta_fixed,
+                   "learned_delta": [int(choices[c - 2]) for c in y_sssp.tolist() if c >= 2]}
+    out["both_speedup"] = (t_bf + t_sf) / (t_bl + t_sl)
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -337,29 +380,45 @@ def run_ours(args):
              "sssp_stored_u255_gteps": qst["edges"] / (qst["total_ms"] * 1e-3) / 1e9,
              "bfs_ms_per_64": bfs_ms, "sssp_ms_per_64": sssp_ms}
 
+    # learned vs fixed schedule on this graph (same sources, identical results required)
+    if not args.no_schedule:
+        sch = {args.workload: compare_schedules(pkg, d, stream, sb_d, ss_d, lv_d, ds_d, native.WEIGHT_HASH, DELTA, 2)}
+
     # layer builds and update batches (every layer kept exact)
     upd = {}
     if not args.no_updates:
-        def ev_time(fn):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            e0.record(stream)
-            fn()
-            e1.record(stream)
-            e1.synchronize()
-            return e0.elapsed_time(e1)
-        builds = {"wcc_ms": ev_time(lambda: d.build(native.LAYER_WCC)),
-                  "scc_dag_ms": ev_time(lambda: d.build(native.LAYER_SCC)),
-                  "bct_ms": ev_time(lambda: d.build(native.LAYER_BCT))}
+        builds = {"wcc_ms": ev_time(stream, lambda: d.build(native.LAYER_WCC)),
+                  "scc_dag_ms": ev_time(stream, lambda: d.build(native.LAYER_SCC)),
+                  "bct_ms": ev_time(stream, lambda: d.build(native.LAYER_BCT))}
         extra["build"] = builds
         for n in (10_000, 100_000, 1_000_000):
             u, v, ins = pkg.graphs.updates(g, n // 2, n // 2, 50 + n + rank)
             ub, vb, ib = (torch.from_numpy(x).pin_memory() for x in (u, v, ins))
-            t = ev_time(lambda: d.apply_batch(ub.numpy(), vb.numpy(), ib.numpy()))
+            t = ev_time(stream, lambda: d.apply_batch(ub.numpy(), vb.numpy(), ib.numpy()))
             upd[str(n)] = n / (t * 1e-3)
             extra.setdefault("update_phases_ms", {})[str(n)] = {k: round(x, 2) for k, x in d.batch_times().items()}
         extra["updates_per_s"] = upd
+
+    # the high-diameter lattice (4,900 x 4,900, stored Euclidean weights): where the fixed delta
+    # and alpha/beta are far from the best schedule
+    if not args.no_schedule:
+        d.close()
+        del lv_d, ds_d, lv_h, ds_h
+        torch.cuda.empty_cache()
+        gl = pkg.graphs.lattice()
+        d = pkg.DeviceGraph.from_graph(gl)
+        stream = torch.cuda.ExternalStream(d.stream(), device=dev)
+        sl_b = torch.from_numpy(pkg.graphs.sources_with_edges(gl, N_BFS, 21 + 1000 * rank)).to(dev)
+        sl_s = torch.from_numpy(pkg.graphs.sources_with_edges(gl, N_SSSP, 22 + 1000 * rank)).to(dev)
+        lv_l = torch.empty((N_BFS, gl.V), dtype=torch.int32, device=dev)
+        ds_l = torch.empty((N_SSSP, gl.V), dtype=torch.int64, device=dev)
+        res = compare_schedules(pkg, d, stream, sl_b, sl_s, lv_l, ds_l, native.WEIGHT_STORED, DELTA, 1)
+        res["build_wcc_scc_bct_ms"] = ev_time(stream, lambda: d.build(native.LAYER_ALL))
+        res["graph"] = f"lattice 4900 x 4900, 5% removed, 0.1% Pareto(1.5) long-range, V={gl.V}, E={gl.E}"
+        sch["lattice"] = res
+        del lv_l, ds_l
+    if not args.no_schedule:
+        extra["schedule"] = sch
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

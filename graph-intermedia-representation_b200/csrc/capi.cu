@@ -209,6 +209,16 @@ int create_impl(const int32_t* fw_beg, const int32_t* fw_adj, const int32_t* bw_
     GIR_CUDA(g, cudaGetDevice(&g->device));
     GIR_CUDA(g, cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
     GIR_CUDA(g, cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = g->device;
+        GIR_CUDA(g, cudaMemPoolCreate(&g->pool, &props));
+        uint64_t keep = UINT64_MAX;  // memory stays in the pool until the handle is destroyed
+        GIR_CUDA(g, cudaMemPoolSetAttribute(g->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     GIR_CUDA(g, cudaEventCreate(&g->ev0));
     GIR_CUDA(g, cudaEventCreate(&g->ev1));
     GIR_CUDA(g, cudaEventCreate(&g->ev2));
@@ -222,7 +232,7 @@ int create_impl(const int32_t* fw_beg, const int32_t* fw_adj, const int32_t* bw_
     DevBuf fb, fa, bb, ba, wb;
     const void *d_fb, *d_fa, *d_bb, *d_ba, *d_w = nullptr;
     int rc = GIR_OK;
-    auto cleanup = [&]() { release(fb); release(fa); release(bb); release(ba); release(wb); };
+    auto cleanup = [&]() { release(g, fb); release(g, fa); release(g, bb); release(g, ba); release(g, wb); };
     if ((rc = stage_input(g, fb, fw_beg, sizeof(int32_t) * (V + 1), &d_fb)) ||
         (rc = stage_input(g, fa, fw_adj, sizeof(int32_t) * E, &d_fa)) ||
         (rc = stage_input(g, bb, bw_beg, sizeof(int32_t) * (V + 1), &d_bb)) ||
@@ -254,7 +264,7 @@ int create_impl(const int32_t* fw_beg, const int32_t* fw_adj, const int32_t* bw_
         return rc;
     }
     cleanup();
-    for (auto& b : g->work) release(b);
+    for (auto& b : g->work) release(g, b);
     if (e_fw != e_bw)
         return fail(g, GIR_ERR_MALFORMED, "forward and backward CSR disagree after deduplication (" +
                                               std::to_string(e_fw) + " vs " + std::to_string(e_bw) + " edges)");
@@ -296,10 +306,11 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     for (double& x : g->b_ms) x = 0;
     const double t_start = now_ms();
     if (n <= 0) return GIR_OK;
+    trace_mark(g, "batch: start");
     const void *du, *dv, *dins;
     DevBuf su, sv, si;
     int rc = GIR_OK;
-    auto cleanup = [&]() { release(su); release(sv); release(si); };
+    auto cleanup = [&]() { release(g, su); release(g, sv); release(g, si); };
     if ((rc = stage_input(g, su, u, sizeof(int32_t) * n, &du)) || (rc = stage_input(g, sv, v, sizeof(int32_t) * n, &dv)) ||
         (rc = stage_input(g, si, ins, n, &dins))) {
         cleanup();
@@ -343,6 +354,7 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     g->b_ins = n_ins;
     g->b_del = n_del;
     if (n_ins + n_del == 0) return GIR_OK;
+    trace_mark(g, "batch: normalize");
 
     // undirected pairs touched, with their presence before the batch
     const int64_t np = n_ins + n_del;
@@ -366,8 +378,10 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     k_pair_presence<<<grid_for(g, npu, kBlock), kBlock, 0, g->stream>>>(pairs, npu, view(g->fw), V, before);
     GIR_LAUNCH(g, "k_pair_presence");
 
+    trace_mark(g, "batch: pairs");
     // forward, then backward (transposed keys, re-sorted)
     GIR_TRY(store_apply_ops(g, g->fw, ins_k, n_ins, del_k, n_del, true));
+    trace_mark(g, "batch: forward ops");
     GIR_TRY(ensure_n(g, g->work[4], np + 2, &tk));
     uint64_t* tk2 = tk + n_ins + 1;
     if (n_ins) {
@@ -381,6 +395,7 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
         GIR_TRY(sort_keys_u64(g, tk2, del_k, n_del, 64));
     }
     GIR_TRY(store_apply_ops(g, g->bw, tk, n_ins, tk2, n_del, false));
+    trace_mark(g, "batch: backward ops");
 
     // symmetrized view: pairs whose undirected presence changed
     k_sym_ops<<<grid_for(g, npu, kBlock), kBlock, 0, g->stream>>>(pairs, npu, before, view(g->fw), V, sym_keys, fsi, fsd);
@@ -393,6 +408,7 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     GIR_TRY(sort_keys_u64(g, sym_ins, sym_keys, nsi, 64));
     GIR_TRY(sort_keys_u64(g, sym_del, sym_keys, nsd, 64));
     GIR_TRY(store_apply_ops(g, g->sym, sym_ins, nsi, sym_del, nsd, false));
+    trace_mark(g, "batch: symmetric ops");
 
     GIR_TRY(invalidate_after_update(g));
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
@@ -530,16 +546,18 @@ int gir_dev_load(const char* dir, gir_dev_t** out) {
 
 int gir_dev_destroy(gir_dev_t* g) {
     if (!g) return GIR_OK;
+    if (g->stream && g->pool) {
+        store_free(g, g->fw); store_free(g, g->bw); store_free(g, g->sym);
+        store_free(g, g->ws[0]); store_free(g, g->ws[1]);
+        for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
+                          &g->cub_tmp, &g->stage_in, &g->stage_out, &g->sched_w, &g->sched_io, &g->lane_dist})
+            release(g, *b);
+        for (auto& b : g->scratch) release(g, b);
+        for (auto& b : g->work) release(g, b);
+        for (auto& b : g->qitems) release(g, b);
+    }
     if (g->stream) cudaStreamSynchronize(g->stream);
-    store_free(g->fw); store_free(g->bw); store_free(g->sym);
-    store_free(g->ws[0]); store_free(g->ws[1]);
-    release(g->wcc); release(g->scc); release(g->scc_rank); release(g->dag);
-    release(g->blk_label); release(g->blk_head); release(g->bcnt); release(g->bins);
-    for (auto& b : g->scratch) release(b);
-    for (auto& b : g->work) release(b);
-    release(g->cub_tmp); release(g->stage_in); release(g->stage_out); release(g->sched_w);
-    release(g->sched_io); release(g->lane_dist);
-    for (auto& b : g->qitems) release(b);
+    if (g->pool) cudaMemPoolDestroy(g->pool);
     if (g->pinned) cudaFreeHost(g->pinned);
     for (cudaEvent_t e : {g->ev0, g->ev1, g->ev2, g->ev3, g->pev0, g->pev1}) if (e) cudaEventDestroy(e);
     if (g->stream) cudaStreamDestroy(g->stream);
@@ -658,7 +676,7 @@ int gir_dev_has_edges(gir_dev_t* g, int undirected, const int32_t* u, const int3
     if (!rc) rc = out_target(g, out, (size_t)n, g->stage_out, &dout);
     if (!rc) rc = store_has_edges(g, undirected ? g->sym : g->fw, (const int32_t*)du, (const int32_t*)dv, n, (uint8_t*)dout);
     if (!rc) rc = finish_out(g, out, dout, (size_t)n);
-    release(su); release(sv);
+    release(g, su); release(g, sv);
     return rc;
 }
 

@@ -108,6 +108,11 @@ struct gir_dev {
     int64_t bin_n[3] = {0, 0, 0};
     bool bins_valid = false;
 
+    // Stream-ordered pool of every device buffer of the handle: allocations and frees are queued
+    // on the handle's stream and the pool keeps its memory, so no call waits for the device to
+    // go idle the way cudaMalloc / cudaFree do.
+    cudaMemPool_t pool = nullptr;
+
     // Scratch, grown on demand and kept across calls.
     gir::DevBuf scratch[16];
     gir::DevBuf cub_tmp;
@@ -158,6 +163,14 @@ double now_ms();
 // With tracing on: synchronizes the handle's stream, prints `what` and the ms since the last mark.
 void trace_mark(gir_dev* g, const char* what);
 
+// Device memory from the handle's pool, ordered on its stream.
+int dev_alloc(gir_dev* g, void** p, size_t bytes);
+template <class T>
+int dev_alloc_n(gir_dev* g, T** p, size_t n) {
+    return dev_alloc(g, reinterpret_cast<void**>(p), n * sizeof(T));
+}
+void dev_free(gir_dev* g, void* p);
+
 // Grows a device buffer to at least `bytes` (contents not kept).
 int ensure(gir_dev* g, DevBuf& b, size_t bytes);
 template <class T>
@@ -166,7 +179,7 @@ int ensure_n(gir_dev* g, DevBuf& b, size_t n, T** out) {
     *out = static_cast<T*>(b.p);
     return GIR_OK;
 }
-void release(DevBuf& b);
+void release(gir_dev* g, DevBuf& b);
 
 // Pinned host scratch of at least `bytes`.
 int pinned(gir_dev* g, size_t bytes, void** out);
@@ -200,7 +213,7 @@ int MainTimer::run(F&& launch) {
 
 // ---- store (store.cu) ----
 int store_build_csr_from_keys(gir_dev* g, DevCSR& c, const uint64_t* keys, int64_t n, const uint32_t* w);
-int store_free(DevCSR& c);
+int store_free(gir_dev* g, DevCSR& c);
 int store_build_sym(gir_dev* g);
 int store_compact_csr(gir_dev* g, const DevCSR& c, int64_t* beg_out, int32_t* adj_out, int64_t cap);
 int store_has_edges(gir_dev* g, const DevCSR& c, const int32_t* u, const int32_t* v, int64_t n, uint8_t* out);

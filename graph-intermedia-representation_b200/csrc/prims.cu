@@ -20,26 +20,39 @@ int cuda_check(gir_dev* g, cudaError_t e, const char* what) {
     return fail(g, code, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-int ensure(gir_dev* g, DevBuf& b, size_t bytes) {
-    if (b.bytes >= bytes && b.p) return GIR_OK;
-    const double t0 = g->trace_on ? now_ms() : 0.0;
-    if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
-    size_t want = bytes < 256 ? 256 : bytes;
-    want = (want + 255) & ~(size_t)255;
-    cudaError_t e = cudaMalloc(&b.p, want);
-    if (g->trace_on) std::fprintf(stderr, "[gir] alloc %zu bytes: %.3f ms\n", want, now_ms() - t0);
+int dev_alloc(gir_dev* g, void** p, size_t bytes) {
+    *p = nullptr;
+    const size_t want = ((bytes < 256 ? 256 : bytes) + 255) & ~(size_t)255;
+    const cudaError_t e = cudaMallocFromPoolAsync(p, want, g->pool, g->stream);
     if (e != cudaSuccess) {
-        b.p = nullptr;
+        *p = nullptr;
         cudaGetLastError();
         return fail(g, GIR_ERR_OOM, "device allocation of " + std::to_string(want) + " bytes failed: " +
                                         cudaGetErrorString(e));
     }
+    return GIR_OK;
+}
+
+void dev_free(gir_dev* g, void* p) {
+    if (p) cudaFreeAsync(p, g->stream);
+}
+
+int ensure(gir_dev* g, DevBuf& b, size_t bytes) {
+    if (b.bytes >= bytes && b.p) return GIR_OK;
+    const double t0 = g->trace_on ? now_ms() : 0.0;
+    // a buffer that has to grow again gets a quarter more than asked, so sizes that creep up
+    // (capacities after relayouts, batch sizes) do not reallocate every call
+    size_t want = b.p ? bytes + bytes / 4 : bytes;
+    want = ((want < 256 ? 256 : want) + 255) & ~(size_t)255;
+    release(g, b);
+    GIR_TRY(dev_alloc(g, &b.p, want));
+    if (g->trace_on) std::fprintf(stderr, "[gir] alloc %zu bytes: %.3f ms\n", want, now_ms() - t0);
     b.bytes = want;
     return GIR_OK;
 }
 
-void release(DevBuf& b) {
-    if (b.p) cudaFree(b.p);
+void release(gir_dev* g, DevBuf& b) {
+    dev_free(g, b.p);
     b.p = nullptr;
     b.bytes = 0;
 }

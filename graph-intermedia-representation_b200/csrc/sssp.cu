@@ -384,13 +384,13 @@ __global__ void k_transpose(const uint64_t* dist, int64_t V, int nl, uint64_t* o
 // Weight-sorted copy of the forward CSR for one weight mode (compact rows).
 static int build_weight_sorted(gir_dev* g, int hash, DevCSR& ws) {
     const int64_t V = g->V, E = g->fw.E;
-    store_free(ws);
+    store_free(g, ws);
     uint64_t *keys = nullptr, *ktmp = nullptr;
     uint32_t *cols = nullptr, *ctmp = nullptr;
-    GIR_CUDA(g, cudaMalloc(&ws.beg, sizeof(int64_t) * (V + 1)));
-    GIR_CUDA(g, cudaMalloc(&ws.deg, sizeof(int32_t) * (V > 0 ? V : 1)));
-    GIR_CUDA(g, cudaMalloc(&ws.adj, sizeof(int32_t) * (E > 0 ? E : 1)));
-    GIR_CUDA(g, cudaMalloc(&ws.w, sizeof(uint32_t) * (E > 0 ? E : 1)));
+    GIR_TRY(dev_alloc_n(g, &ws.beg, V + 1));
+    GIR_TRY(dev_alloc_n(g, &ws.deg, V > 0 ? V : 1));
+    GIR_TRY(dev_alloc_n(g, &ws.adj, E > 0 ? E : 1));
+    GIR_TRY(dev_alloc_n(g, &ws.w, E > 0 ? E : 1));
     ws.cap = ws.E = E;
     int64_t* cb = ws.beg;
     k_deg_i64<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, g->fw.deg, cb);

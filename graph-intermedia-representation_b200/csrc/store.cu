@@ -269,11 +269,11 @@ __global__ void k_bin_flags(int64_t V, const int32_t* deg, int32_t small, int32_
 
 }  // namespace
 
-int store_free(DevCSR& c) {
-    if (c.beg) cudaFree(c.beg);
-    if (c.deg) cudaFree(c.deg);
-    if (c.adj) cudaFree(c.adj);
-    if (c.w) cudaFree(c.w);
+int store_free(gir_dev* g, DevCSR& c) {
+    dev_free(g, c.beg);
+    dev_free(g, c.deg);
+    dev_free(g, c.adj);
+    dev_free(g, c.w);
     c = DevCSR{};
     return GIR_OK;
 }
@@ -281,15 +281,15 @@ int store_free(DevCSR& c) {
 int store_build_csr_from_keys(gir_dev* g, DevCSR& c, const uint64_t* keys, int64_t n, const uint32_t* kw) {
     // keys: sorted, distinct (row << 32 | col). kw (nullable): weight per key.
     const int64_t V = g->V;
-    store_free(c);
+    store_free(g, c);
     int64_t *first = nullptr, *endp = nullptr, *capv = nullptr;
     GIR_TRY(ensure_n(g, g->scratch[10], V + 1, &first));
     GIR_TRY(ensure_n(g, g->scratch[11], V + 1, &endp));
     GIR_TRY(ensure_n(g, g->scratch[12], V + 1, &capv));
     GIR_CUDA(g, cudaMemsetAsync(first, 0, sizeof(int64_t) * (V + 1), g->stream));
     GIR_CUDA(g, cudaMemsetAsync(endp, 0, sizeof(int64_t) * (V + 1), g->stream));
-    GIR_CUDA(g, cudaMalloc(&c.beg, sizeof(int64_t) * (V + 1)));
-    GIR_CUDA(g, cudaMalloc(&c.deg, sizeof(int32_t) * (V > 0 ? V : 1)));
+    GIR_TRY(dev_alloc_n(g, &c.beg, V + 1));
+    GIR_TRY(dev_alloc_n(g, &c.deg, V > 0 ? V : 1));
     if (n > 0) {
         k_row_runs<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(keys, n, first, endp);
         GIR_LAUNCH(g, "k_row_runs");
@@ -301,8 +301,8 @@ int store_build_csr_from_keys(gir_dev* g, DevCSR& c, const uint64_t* keys, int64
     int64_t total = 0;
     GIR_CUDA(g, cudaMemcpyAsync(&total, c.beg + V, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-    GIR_CUDA(g, cudaMalloc(&c.adj, sizeof(int32_t) * (total > 0 ? total : 4)));
-    if (kw) GIR_CUDA(g, cudaMalloc(&c.w, sizeof(uint32_t) * (total > 0 ? total : 4)));
+    GIR_TRY(dev_alloc_n(g, &c.adj, total > 0 ? total : 4));
+    if (kw) GIR_TRY(dev_alloc_n(g, &c.w, total > 0 ? total : 4));
     c.cap = total;
     c.E = n;
     if (n > 0) {
@@ -433,6 +433,7 @@ int store_apply_ops(gir_dev* g, DevCSR& c, const uint64_t* ins, int64_t n_ins, c
         GIR_LAUNCH(g, "k_set_deg");
     } else {
         // Some row outgrew its slack: new layout for the whole CSR.
+        trace_mark(g, "store: merge before relayout");
         int32_t* slot = nullptr;
         int64_t* capv = nullptr;
         GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &slot));
@@ -446,21 +447,23 @@ int store_apply_ops(gir_dev* g, DevCSR& c, const uint64_t* ins, int64_t n_ins, c
         k_new_caps<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, c.deg, capv);
         GIR_LAUNCH(g, "k_new_caps");
         int64_t* nbeg = nullptr;
-        GIR_CUDA(g, cudaMalloc(&nbeg, sizeof(int64_t) * (V + 1)));
+        GIR_TRY(dev_alloc_n(g, &nbeg, V + 1));
         GIR_TRY(exclusive_scan_i64(g, capv, nbeg, V + 1));
         int64_t total = 0;
         GIR_CUDA(g, cudaMemcpyAsync(&total, nbeg + V, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
         GIR_CUDA(g, cudaStreamSynchronize(g->stream));
         int32_t* nadj = nullptr;
         uint32_t* nw = nullptr;
-        GIR_CUDA(g, cudaMalloc(&nadj, sizeof(int32_t) * (total > 0 ? total : 4)));
-        if (c.w) GIR_CUDA(g, cudaMalloc(&nw, sizeof(uint32_t) * (total > 0 ? total : 4)));
+        GIR_TRY(dev_alloc_n(g, &nadj, total > 0 ? total : 4));
+        if (c.w) GIR_TRY(dev_alloc_n(g, &nw, total > 0 ? total : 4));
         k_relayout_rows<<<grid_for(g, V * 32, kBlock), kBlock, 0, g->stream>>>(V, c.beg, c.adj, c.w, c.deg, nbeg, nadj,
                                                                                  nw, slot, noff, tmp, tmpw);
         GIR_LAUNCH(g, "k_relayout_rows");
-        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-        cudaFree(c.beg); cudaFree(c.adj); if (c.w) cudaFree(c.w);
+        dev_free(g, c.beg);
+        dev_free(g, c.adj);
+        dev_free(g, c.w);
         c.beg = nbeg; c.adj = nadj; c.w = nw; c.cap = total;
+        trace_mark(g, "store: relayout");
     }
     c.E += n_ins - n_del;
     return GIR_OK;

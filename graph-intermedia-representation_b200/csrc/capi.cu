@@ -270,7 +270,28 @@ int create_impl(const int32_t* fw_beg, const int32_t* fw_adj, const int32_t* bw_
                                               std::to_string(e_fw) + " vs " + std::to_string(e_bw) + " edges)");
     g->has_weights = w != nullptr;
     GIR_TRY(store_build_sym(g));
+    // Prime the pool with one block the size of the layer builds' largest working set (sort keys
+    // and their double buffers over the symmetrized capacity), so the first build and the first
+    // large batch do not map new memory piece by piece. At most a quarter of the free memory.
+    {
+        size_t free_b = 0, total_b = 0;
+        GIR_CUDA(g, cudaMemGetInfo(&free_b, &total_b));
+        uint64_t reserved = 0;
+        GIR_CUDA(g, cudaMemPoolGetAttribute(g->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+        size_t want = (size_t)(24 * g->sym.cap + 64 * V);
+        want = want < free_b / 4 ? want : free_b / 4;
+        if (want > reserved) {
+            void* p = nullptr;
+            GIR_TRY(dev_alloc(g, &p, want - reserved));
+            dev_free(g, p);
+        }
+    }
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    if (g->trace_on) {
+        uint64_t r = 0;
+        cudaMemPoolGetAttribute(g->pool, cudaMemPoolAttrReservedMemCurrent, &r);
+        std::fprintf(stderr, "[gir] pool reserved after create: %.1f MB\n", r / 1e6);
+    }
     return GIR_OK;
 }
 
@@ -557,6 +578,12 @@ int gir_dev_destroy(gir_dev_t* g) {
         for (auto& b : g->qitems) release(g, b);
     }
     if (g->stream) cudaStreamSynchronize(g->stream);
+    if (g->pool && g->trace_on) {
+        uint64_t hi = 0, used_hi = 0;
+        cudaMemPoolGetAttribute(g->pool, cudaMemPoolAttrReservedMemHigh, &hi);
+        cudaMemPoolGetAttribute(g->pool, cudaMemPoolAttrUsedMemHigh, &used_hi);
+        std::fprintf(stderr, "[gir] pool high-water: reserved %.1f MB, used %.1f MB\n", hi / 1e6, used_hi / 1e6);
+    }
     if (g->pool) cudaMemPoolDestroy(g->pool);
     if (g->pinned) cudaFreeHost(g->pinned);
     for (cudaEvent_t e : {g->ev0, g->ev1, g->ev2, g->ev3, g->pev0, g->pev1}) if (e) cudaEventDestroy(e);

@@ -27,7 +27,8 @@ constexpr int kChunk = 32 * 16;  // edge positions per warp in the top-down expa
 
 // counters: [0] queue length, [1] (vertex, lane) pairs reached this iteration,
 //           [2] out-edges of those pairs, [3] candidates queued by top-down
-enum { C_Q = 0, C_PAIRS = 1, C_MEDGES = 2, C_CAND = 3, C_N = 4 };
+// [4] the device-decided direction of the next level and [5..8] its features (learned schedule)
+enum { C_Q = 0, C_PAIRS = 1, C_MEDGES = 2, C_CAND = 3, C_DIR = 4, C_FEAT = 5, C_N = 9 };
 
 __device__ __forceinline__ void write_levels(int32_t* level, int64_t V, int32_t v, uint64_t nb, int32_t L) {
     while (nb) {
@@ -68,9 +69,10 @@ __global__ void k_frontier_degrees(const int32_t* q, int64_t nq, const int32_t* 
 
 // Top-down: warp w takes edge positions [w*kChunk, (w+1)*kChunk) of the frontier's out-edges
 // (pref = exclusive scan of frontier degrees).
-__global__ void k_td_expand(const int32_t* q, int64_t nq, const int64_t* pref, int64_t total, CSRView fw,
+__global__ void k_td_expand(const int32_t* q, int64_t nq, const int64_t* pref, CSRView fw,
                             const uint64_t* front, const uint64_t* seen, uint64_t* next, int32_t* cand,
                             unsigned long long* cnt) {
+    const int64_t total = pref[nq];  // (read here, so the host needs no copy of it)
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -105,9 +107,10 @@ __global__ void k_clear_front(const int32_t* q, int64_t nq, uint64_t* front) {
 }
 
 // Top-down commit: candidates become the new frontier with their newly reached lanes.
-__global__ void k_td_commit(const int32_t* cand, int64_t nc, uint64_t* seen, uint64_t* front, uint64_t* next,
-                            const int32_t* outdeg, int32_t* level, int64_t V, int32_t L, int32_t* q,
+__global__ void k_td_commit(const unsigned long long* n_cand, const int32_t* cand, uint64_t* seen, uint64_t* front,
+                            uint64_t* next, const int32_t* outdeg, int32_t* level, int64_t V, int32_t L, int32_t* q,
                             unsigned long long* cnt) {
+    const int64_t nc = (int64_t)*n_cand;
     unsigned long long pairs = 0, medges = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nc; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
@@ -340,10 +343,14 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
         GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
         GIR_CUDA(g, cudaStreamSynchronize(g->stream));
         int64_t nq = (int64_t)hc[0];
+        const bool learned = g->schedule == GIR_SCHEDULE_LEARNED && g->sched_loaded && V >= 4096;
         if (nq > 0) {
             k_source_edges<<<grid_for(g, nq, kBlock), kBlock, 0, g->stream>>>(qa, nq, front, g->fw.deg, cnt);
             GIR_LAUNCH(g, "k_source_edges");
             st.launches++;
+            if (learned)
+                GIR_TRY(sched_bfs_decide_async(g, cnt, C_PAIRS, C_MEDGES, C_DIR, C_FEAT, nl, (double)E, false, alpha,
+                                               beta));
             GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
             GIR_CUDA(g, cudaStreamSynchronize(g->stream));
         }
@@ -356,17 +363,14 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
         int32_t L = 0;
         while (nq > 0) {
             // direction (the reference's switch, gir_query.cpp:159-169, or the schedule network)
-            if (V >= 4096) {
+            if (learned) {  // decided on the device with the counters just read
+                bottom_up = hc[C_DIR] != 0;
+                sched_trace(g, reinterpret_cast<const float*>(&hc[C_FEAT]), bottom_up ? 1 : 0);
+            } else if (V >= 4096) {
                 float feat[GIR_SCHED_IN];
                 sched_bfs_features(g, nf, mf, mu, L, bottom_up, nl, feat);
-                if (g->schedule == GIR_SCHEDULE_LEARNED && g->sched_loaded) {
-                    int bu = bottom_up;
-                    GIR_TRY(sched_choose_direction(g, feat, bottom_up, &bu));
-                    bottom_up = bu != 0;
-                } else {
-                    if (!bottom_up && mf * alpha > mu) bottom_up = true;
-                    else if (bottom_up && nf * beta < (double)V) bottom_up = false;
-                }
+                if (!bottom_up && mf * alpha > mu) bottom_up = true;
+                else if (bottom_up && nf * beta < (double)V) bottom_up = false;
                 sched_trace(g, feat, bottom_up ? 1 : 0);
             }
             GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
@@ -378,32 +382,25 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
                 k_frontier_degrees<<<grid_for(g, nq, kBlock), kBlock, 0, g->stream>>>(qa, nq, g->fw.deg, pref);
                 GIR_LAUNCH(g, "k_frontier_degrees");
                 GIR_TRY(exclusive_scan_i64(g, pref, pref, nq + 1));
-                int64_t total = 0;
-                GIR_CUDA(g, cudaMemcpyAsync(&hc[8], pref + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
-                GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-                total = (int64_t)hc[8];
-                if (total > 0) {
-                    const int64_t chunks = (total + kChunk - 1) / kChunk;
-                    const int64_t warps_per_block = kBlock / 32;
-                    int64_t blocks = (chunks + warps_per_block - 1) / warps_per_block;
-                    if (blocks > grid) blocks = grid;
-                    GIR_TRY(timer.run([&]() -> int {
-                        k_td_expand<<<(int)blocks, kBlock, 0, g->stream>>>(qa, nq, pref, total, view(g->fw), front,
-                                                                           seen, next, qb, cnt);
-                        GIR_LAUNCH(g, "k_td_expand");
-                        return GIR_OK;
-                    }));
-                }
+                // The frontier's row total and the candidate count stay on the device: the
+                // kernels are sized from the host's upper bound (the frontier's out-edges over
+                // all lanes, counted at the end of the previous level) and read the exact ones.
+                const double bound = std::min(mf * nl, (double)E) + 1.0;
+                const int64_t warps_per_block = kBlock / 32;
+                int64_t blocks = (int64_t)((bound / kChunk + warps_per_block) / warps_per_block) + 1;
+                if (blocks > grid) blocks = grid;
+                GIR_TRY(timer.run([&]() -> int {
+                    k_td_expand<<<(int)blocks, kBlock, 0, g->stream>>>(qa, nq, pref, view(g->fw), front, seen, next, qb,
+                                                                       cnt);
+                    GIR_LAUNCH(g, "k_td_expand");
+                    return GIR_OK;
+                }));
                 k_clear_front<<<grid_for(g, nq, kBlock), kBlock, 0, g->stream>>>(qa, nq, front);
                 GIR_LAUNCH(g, "k_clear_front");
-                GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
-                GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-                const int64_t nc = (int64_t)hc[C_CAND];
-                if (nc > 0) {
-                    k_td_commit<<<grid_for(g, nc, kBlock), kBlock, 0, g->stream>>>(qb, nc, seen, front, next, g->fw.deg,
-                                                                                   level, V, L + 1, qa, cnt);
-                    GIR_LAUNCH(g, "k_td_commit");
-                }
+                const int64_t nc_bound = (int64_t)std::min(bound, (double)V);
+                k_td_commit<<<grid_for(g, nc_bound, kBlock), kBlock, 0, g->stream>>>(
+                    cnt + C_CAND, qb, seen, front, next, g->fw.deg, level, V, L + 1, qa, cnt);
+                GIR_LAUNCH(g, "k_td_commit");
                 st.launches += 4;
             } else {
                 const int32_t* bins = static_cast<const int32_t*>(g->bins.p);
@@ -435,6 +432,8 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
                 next_dirty = true;
                 st.bottom_up++;
             }
+            if (learned)
+                GIR_TRY(sched_bfs_decide_async(g, cnt, C_PAIRS, C_MEDGES, C_DIR, C_FEAT, nl, mu, bottom_up, alpha, beta));
             GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
             GIR_CUDA(g, cudaStreamSynchronize(g->stream));
             nq = (int64_t)hc[C_Q];

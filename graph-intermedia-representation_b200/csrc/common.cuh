@@ -247,7 +247,11 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
 
 // ---- schedule network (sched.cu) ----
 int sched_choose_delta(gir_dev* g, const float* features, uint64_t* delta);
-int sched_choose_direction(gir_dev* g, const float* features, int current, int* bottom_up);
+// Enqueues the device decision of the next BFS level's direction: reads the frontier's pairs and
+// out-edges at cnt[i_pairs] / cnt[i_medges], writes the direction (0 top-down, 1 bottom-up) to
+// cnt[i_dir] and the GIR_SCHED_IN features (floats) from cnt[i_feat] on.
+int sched_bfs_decide_async(gir_dev* g, unsigned long long* cnt, int i_pairs, int i_medges, int i_dir, int i_feat,
+                           int lanes, double mu_prev, bool bottom_up, double alpha, double beta);
 // Feature rows (GIR_SCHED_IN floats) of the two decisions. BFS level: frontier vertices and
 // out-edges, unexplored out-edges, level, current direction, graph density, lanes. SSSP group:
 // density, mean / max weight, size, lanes.

@@ -7,10 +7,16 @@
 // gir_query.cpp:161-168; Delta = 16, gir.h:215) are the fallback when no network is loaded.
 //
 // Feature vectors (built by the callers in bfs.cu / sssp.cu, all scaled to O(1)):
-//   BFS level:  [frontier vertices / V, frontier out-edges / E, unexplored out-edges / E,
-//                level / 64, current direction, E / V / 64, lanes / 64, 1]
-//   SSSP query: [E / V / 64, weight kind, SMs / 148, mean weight / 256, max weight / 1024,
-//                0, 0, 1]
+//   BFS level:  [log2(nf / V) / 8, log2(mf / mu) / 8, log2(mu / E) / 8, log2(mf / E) / 8,
+//                current direction, log2(E / V + 1) / 8, lanes / 64, 0]
+//               with nf / mf the frontier's vertices / out-edges and mu the out-edges not yet
+//               explored (per lane). The fixed switch is a threshold on log2(mf / mu) (top-down
+//               -> bottom-up) and on log2(nf / V) (back), so the log scale makes it, and any
+//               better pair of thresholds, a simple function of the inputs.
+//   SSSP query: [log2(E / V + 1) / 8, log2(mean weight + 1) / 16, log2(max weight + 1) / 16,
+//                log2(V) / 32, lanes / 64, 0, 0, 1]
+// A direction is taken from the network only when its two logits differ by at least
+// kDirMargin; otherwise the fixed switch decides.
 // Parameter layout: W1[HID][IN], b1[HID], W2[OUT][HID], b2[OUT].
 #include "common.cuh"
 
@@ -21,7 +27,8 @@ namespace {
 constexpr int IN = GIR_SCHED_IN, HID = GIR_SCHED_HID, OUT = GIR_SCHED_OUT;
 constexpr int NP = HID * IN + HID + OUT * HID + OUT;
 constexpr int kBlock = 128;
-constexpr uint64_t kDeltaChoices[6] = {16, 32, 64, 128, 512, 2048};
+constexpr uint64_t kDeltaChoices[6] = {16, 32, 64, 256, 2048, 8192};
+constexpr float kDirMargin = 2.0f;
 
 struct Layout {
     const float *W1, *b1, *W2, *b2;
@@ -41,6 +48,42 @@ __device__ __forceinline__ void forward_one(const Layout& L, const float* x, flo
         for (int j = 0; j < HID; ++j) z += L.W2[k * HID + j] * h[j];
         o[k] = z;
     }
+}
+
+// BFS level features (the host's sched_bfs_features and the device decision share it).
+__host__ __device__ inline void bfs_features(double V, double E, double nf, double mf, double mu, bool bottom_up,
+                                             int lanes, float* out) {
+    const double tiny = 1.0 / 4294967296.0;
+    out[0] = (float)(log2(nf / V + tiny) / 8.0);
+    out[1] = (float)((log2(mf + 1.0) - log2(mu + 1.0)) / 8.0);
+    out[2] = (float)(log2(mu / E + tiny) / 8.0);
+    out[3] = (float)(log2(mf / E + tiny) / 8.0);
+    out[4] = bottom_up ? 1.f : 0.f;
+    out[5] = (float)(log2(E / V + 1.0) / 8.0);
+    out[6] = (float)(lanes / 64.0);
+    out[7] = 0.f;  // task: BFS direction
+}
+
+// The next BFS level's direction, decided on the device from the level's counters (frontier
+// pairs and out-edges, summed over lanes), so the network costs no extra host round trip: the
+// decision and its features travel back with the counters the host reads anyway.
+__global__ void k_bfs_decide(const float* params, unsigned long long* cnt, int i_pairs, int i_medges, int i_dir,
+                             int i_feat, int lanes, double V, double E, double mu_prev, int bottom_up, double alpha,
+                             double beta, float margin) {
+    if (threadIdx.x != 0) return;
+    const double nf = (double)cnt[i_pairs] / lanes, mf = (double)cnt[i_medges] / lanes;
+    const double mu = mu_prev - mf;
+    float x[IN], h[HID], o[OUT];
+    bfs_features(V, E, nf, mf, mu, bottom_up != 0, lanes, x);
+    int fixed = bottom_up;
+    if (!bottom_up && mf * alpha > mu) fixed = 1;
+    else if (bottom_up && nf * beta < V) fixed = 0;
+    forward_one(layout(params), x, h, o);
+    const int net = o[1] > o[0] ? 1 : 0;
+    const float m = fabsf(o[1] - o[0]);
+    cnt[i_dir] = (unsigned long long)(m >= margin ? net : fixed);
+    float* f = reinterpret_cast<float*>(&cnt[i_feat]);
+    for (int i = 0; i < IN; ++i) f[i] = x[i];
 }
 
 __global__ void k_mlp_forward(const float* params, const float* x, int64_t n, float* logits) {
@@ -146,8 +189,9 @@ int run_grad(gir_dev* g, const float* x_dev, const int32_t* y_dev, int64_t n, fl
     return GIR_OK;
 }
 
-// One decision: logits of one feature vector, argmax over [lo, hi).
-int decide(gir_dev* g, const float* features, int lo, int hi, int* choice) {
+// One decision: logits of one feature vector, argmax over [lo, hi) and its margin over the
+// runner-up.
+int decide(gir_dev* g, const float* features, int lo, int hi, int* choice, float* margin) {
     float* buf = nullptr;
     GIR_TRY(ensure_n(g, g->sched_io, IN + OUT + 8, &buf));
     float tmp_in[IN];
@@ -160,7 +204,11 @@ int decide(gir_dev* g, const float* features, int lo, int hi, int* choice) {
     int best = lo;
     for (int k = lo + 1; k < hi; ++k)
         if (logits[k] > logits[best]) best = k;
+    float second = -3.0e38f;
+    for (int k = lo; k < hi; ++k)
+        if (k != best && logits[k] > second) second = logits[k];
     *choice = best;
+    *margin = logits[best] - second;
     return GIR_OK;
 }
 
@@ -168,15 +216,19 @@ int decide(gir_dev* g, const float* features, int lo, int hi, int* choice) {
 
 void sched_bfs_features(const gir_dev* g, double nf, double mf, double mu, int level, bool bottom_up, int lanes,
                         float* out) {
-    const double V = (double)(g->V > 0 ? g->V : 1), E = (double)g->fw.E + 1.0;
-    out[0] = (float)(nf / V);
-    out[1] = (float)(mf / E);
-    out[2] = (float)(mu / E);
-    out[3] = (float)((level < 64 ? level : 64) / 64.0);
-    out[4] = bottom_up ? 1.f : 0.f;
-    out[5] = (float)(std::log2(E / V + 1.0) / 8.0);
-    out[6] = (float)(lanes / 64.0);
-    out[7] = 0.f;  // task: BFS direction
+    (void)level;
+    bfs_features((double)(g->V > 0 ? g->V : 1), (double)g->fw.E + 1.0, nf, mf, mu, bottom_up, lanes, out);
+}
+
+int sched_bfs_decide_async(gir_dev* g, unsigned long long* cnt, int i_pairs, int i_medges, int i_dir, int i_feat,
+                           int lanes, double mu_prev, bool bottom_up, double alpha, double beta) {
+    float* p = nullptr;
+    GIR_TRY(ensure_params(g, &p));
+    k_bfs_decide<<<1, 32, 0, g->stream>>>(p, cnt, i_pairs, i_medges, i_dir, i_feat, lanes,
+                                          (double)(g->V > 0 ? g->V : 1), (double)g->fw.E + 1.0, mu_prev,
+                                          bottom_up ? 1 : 0, alpha, beta, kDirMargin);
+    GIR_LAUNCH(g, "k_bfs_decide");
+    return GIR_OK;
 }
 
 void sched_sssp_features(const gir_dev* g, int weight_mode, int lanes, float* out) {
@@ -208,17 +260,10 @@ void sched_trace(gir_dev* g, const float* x, int32_t y) {
     g->trace_y.push_back(y);
 }
 
-int sched_choose_direction(gir_dev* g, const float* features, int current, int* bottom_up) {
-    (void)current;
-    int c = 0;
-    GIR_TRY(decide(g, features, 0, 2, &c));
-    *bottom_up = c == 1;
-    return GIR_OK;
-}
-
 int sched_choose_delta(gir_dev* g, const float* features, uint64_t* delta) {
     int c = 2;
-    GIR_TRY(decide(g, features, 2, 8, &c));
+    float margin = 0.f;
+    GIR_TRY(decide(g, features, 2, 8, &c, &margin));
     *delta = kDeltaChoices[c - 2];
     return GIR_OK;
 }

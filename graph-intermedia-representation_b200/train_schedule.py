@@ -48,9 +48,11 @@ def suite(pkg, quick):
     out.append((r20, "stored"))
     out.append((G.lattice(side=300, seed=41), "stored"))
     if not quick:
-        out.append((G.rmat_lj(), "hash"))
-        out.append((G.rmat_lj(), "stored"))
+        lj = G.rmat_lj()
+        out.append((lj, "hash"))
+        out.append((lj, "stored"))
         out.append((G.lattice(side=800, seed=42), "stored"))
+        out.append((G.lattice(side=1500, seed=43), "stored"))
     return out
 
 
@@ -94,8 +96,8 @@ def main():
                 src = torch.from_numpy(pkg.graphs.sources_with_edges(g, lanes, 9 + lanes)).to("cuda:0")
                 out = torch.empty((lanes, g.V), dtype=torch.int32, device="cuda:0")
                 res = []
-                for alpha in (2.0, 8.0, 15.0, 40.0, 150.0):
-                    for beta in (4.0, 18.0, 80.0):
+                for alpha in (2.0, 6.0, 15.0, 40.0, 150.0, 600.0):
+                    for beta in (2.0, 6.0, 18.0, 80.0, 300.0):
                         d.set_param(native.PARAM_ALPHA, alpha)
                         d.set_param(native.PARAM_BETA, beta)
                         res.append((timed(lambda: d.bfs(src, out=out)), alpha, beta))

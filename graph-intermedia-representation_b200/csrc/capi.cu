@@ -295,24 +295,89 @@ int create_impl(const int32_t* fw_beg, const int32_t* fw_adj, const int32_t* bw_
     return GIR_OK;
 }
 
+// What a batch can change in the layers, judged with the labels from before it (flags in
+// cnt[F_*]); the classes are exact sufficient conditions for keeping a layer, anything else
+// rebuilds it:
+//  - SCC labels stay when no edge inside an SCC is deleted and every inserted edge between
+//    SCCs goes forward in the rank order (rank(u) < rank(v) for u -> v: the ranks are a
+//    topological order of the condensation, which such an edge keeps acyclic). The DAG then
+//    changes only if a cross edge was inserted or deleted;
+//  - blocks stay when the SCCs stay and every changed symmetric pair either joins two SCCs
+//    (not an edge of H) or is an inserted pair whose endpoints already share a block (a
+//    block's vertices are those with it as parent block plus its head).
+enum { F_SCC_SPLIT = 4, F_SCC_CYCLE = 5, F_DAG = 6, F_BCT = 7, F_N = 8 };
+
+__global__ void k_classify_directed(const uint64_t* ins, int64_t n_ins, const uint64_t* del, int64_t n_del,
+                                    const int32_t* scc, const int32_t* rank, unsigned long long* cnt) {
+    bool split = false, cycle = false, dag = false;
+    GRID_STRIDE(i, n_ins + n_del) {
+        const bool is_ins = i < n_ins;
+        const uint64_t k = is_ins ? ins[i] : del[i - n_ins];
+        const int32_t u = (int32_t)(k >> 32), v = (int32_t)(k & 0xffffffffULL);
+        if (scc[u] == scc[v]) {
+            split |= !is_ins;
+        } else {
+            dag = true;
+            cycle |= is_ins && rank[u] >= rank[v];
+        }
+    }
+    if (split) cnt[F_SCC_SPLIT] = 1;
+    if (cycle) cnt[F_SCC_CYCLE] = 1;
+    if (dag) cnt[F_DAG] = 1;
+}
+
+__global__ void k_classify_pairs(const uint64_t* ins, int64_t n_ins, const uint64_t* del, int64_t n_del,
+                                 const int32_t* scc, const int32_t* blk, const int32_t* head,
+                                 unsigned long long* cnt) {
+    bool bct = false;
+    GRID_STRIDE(i, n_ins + n_del) {
+        const bool is_ins = i < n_ins;
+        const uint64_t k = is_ins ? ins[i] : del[i - n_ins];
+        const int32_t u = (int32_t)(k >> 32), w = (int32_t)(k & 0xffffffffULL);
+        if (scc[u] != scc[w]) continue;
+        if (!is_ins) {
+            bct = true;
+        } else {
+            const int32_t bu = blk[u], bw = blk[w];
+            bct |= !(bu == bw || head[bw] == u || head[bu] == w);
+        }
+    }
+    if (bct) cnt[F_BCT] = 1;
+}
+
 int invalidate_after_update(gir_dev* g) {
     g->bins_valid = false;
     g->ws_valid[0] = g->ws_valid[1] = false;
     return GIR_OK;
 }
 
+// Per layer: keep it, patch it (WCC: union the inserted pairs; SCC: DAG and ranks only), or
+// rebuild it.
+enum { KEEP = 0, PATCH = 1, REBUILD = 2 };
+struct RepairPlan {
+    int wcc = REBUILD, scc = REBUILD, bct = REBUILD;
+    const uint64_t* pairs_in = nullptr;  // newly present undirected pairs (both orientations)
+    int64_t n_pairs_in = 0;
+};
+
 // Brings every built layer up to date, timing each (phases 1..3 of gir_dev_batch_times).
-int rebuild_layers(gir_dev* g) {
+int rebuild_layers(gir_dev* g, const RepairPlan& plan) {
     double t = now_ms();
-    if (g->wcc_built) GIR_TRY(wcc_build(g));
+    if (g->wcc_built) {
+        if (plan.wcc == REBUILD) GIR_TRY(wcc_build(g));
+        else if (plan.wcc == PATCH) GIR_TRY(wcc_union_pairs(g, plan.pairs_in, plan.n_pairs_in));
+    }
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     g->b_ms[1] = now_ms() - t;
     t = now_ms();
-    if (g->scc_built) GIR_TRY(scc_build(g));
+    if (g->scc_built) {
+        if (plan.scc == REBUILD) GIR_TRY(scc_build(g));
+        else if (plan.scc == PATCH) GIR_TRY(scc_build_dag(g));
+    }
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     g->b_ms[2] = now_ms() - t;
     t = now_ms();
-    if (g->bct_built) GIR_TRY(bct_build(g));
+    if (g->bct_built && (plan.bct == REBUILD || plan.scc == REBUILD)) GIR_TRY(bct_build(g));
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     g->b_ms[3] = now_ms() - t;
     return GIR_OK;
@@ -325,6 +390,7 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     const int64_t V = g->V;
     g->b_ins = g->b_del = g->b_noop = g->b_invalid = 0;
     for (double& x : g->b_ms) x = 0;
+    for (int& x : g->b_plan) x = 0;  // (a batch without effective ops keeps every layer)
     const double t_start = now_ms();
     if (n <= 0) return GIR_OK;
     trace_mark(g, "batch: start");
@@ -344,12 +410,12 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     if ((rc = ensure_n(g, g->work[0], n + 1, &keys)) || (rc = ensure_n(g, g->work[1], n + 1, &ktmp)) ||
         (rc = ensure_n(g, g->work[2], n + 1, &pos)) || (rc = ensure_n(g, g->work[3], n + 1, &ptmp)) ||
         (rc = ensure_n(g, g->work[4], 2 * n + 2, &f_ins)) || (rc = ensure_n(g, g->work[5], n + 1, &ins_k)) ||
-        (rc = ensure_n(g, g->work[6], n + 1, &del_k)) || (rc = ensure_n(g, g->work[7], 4, &cnt))) {
+        (rc = ensure_n(g, g->work[6], n + 1, &del_k)) || (rc = ensure_n(g, g->work[7], F_N, &cnt))) {
         cleanup();
         return rc;
     }
     f_del = f_ins + n + 1;
-    cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned long long), g->stream);
+    cudaMemsetAsync(cnt, 0, F_N * sizeof(unsigned long long), g->stream);
     k_batch_keys<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>((const int32_t*)du, (const int32_t*)dv, n, V, keys,
                                                                    pos, cnt);
     if ((rc = cuda_check(g, cudaGetLastError(), "k_batch_keys")) ||
@@ -376,6 +442,12 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     g->b_del = n_del;
     if (n_ins + n_del == 0) return GIR_OK;
     trace_mark(g, "batch: normalize");
+    if (g->scc_built) {
+        k_classify_directed<<<grid_for(g, n_ins + n_del, kBlock), kBlock, 0, g->stream>>>(
+            ins_k, n_ins, del_k, n_del, static_cast<const int32_t*>(g->scc.p), static_cast<const int32_t*>(g->scc_rank.p),
+            cnt);
+        GIR_LAUNCH(g, "k_classify_directed");
+    }
 
     // undirected pairs touched, with their presence before the batch
     const int64_t np = n_ins + n_del;
@@ -428,13 +500,30 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     GIR_TRY(select_flagged_u64(g, sym_keys, fsd, sym_del, 2 * npu, &nsd));
     GIR_TRY(sort_keys_u64(g, sym_ins, sym_keys, nsi, 64));
     GIR_TRY(sort_keys_u64(g, sym_del, sym_keys, nsd, 64));
+    if (g->bct_built && nsi + nsd > 0) {
+        k_classify_pairs<<<grid_for(g, nsi + nsd, kBlock), kBlock, 0, g->stream>>>(
+            sym_ins, nsi, sym_del, nsd, static_cast<const int32_t*>(g->scc.p), static_cast<const int32_t*>(g->blk_label.p),
+            static_cast<const int32_t*>(g->blk_head.p), cnt);
+        GIR_LAUNCH(g, "k_classify_pairs");
+    }
     GIR_TRY(store_apply_ops(g, g->sym, sym_ins, nsi, sym_del, nsd, false));
     trace_mark(g, "batch: symmetric ops");
 
     GIR_TRY(invalidate_after_update(g));
+    unsigned long long fl[F_N] = {};
+    GIR_CUDA(g, cudaMemcpyAsync(fl, cnt, sizeof(fl), cudaMemcpyDeviceToHost, g->stream));
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     g->b_ms[0] = now_ms() - t_start;
-    GIR_TRY(rebuild_layers(g));
+    RepairPlan plan;
+    plan.wcc = nsd > 0 ? REBUILD : (nsi > 0 ? PATCH : KEEP);
+    plan.pairs_in = sym_ins;
+    plan.n_pairs_in = nsi;
+    plan.scc = (fl[F_SCC_SPLIT] || fl[F_SCC_CYCLE]) ? REBUILD : (fl[F_DAG] ? PATCH : KEEP);
+    plan.bct = fl[F_BCT] ? REBUILD : KEEP;
+    g->b_plan[0] = plan.wcc;
+    g->b_plan[1] = plan.scc;
+    g->b_plan[2] = plan.scc == REBUILD ? REBUILD : plan.bct;
+    GIR_TRY(rebuild_layers(g, plan));
     return GIR_OK;
 }
 
@@ -749,6 +838,12 @@ int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t h
 int gir_dev_batch_times(gir_dev_t* g, double* ms4) {
     if (!g || !ms4) return GIR_ERR_INVALID;
     for (int i = 0; i < 4; ++i) ms4[i] = g->b_ms[i];
+    return GIR_OK;
+}
+
+int gir_dev_batch_plan(gir_dev_t* g, int32_t* plan3) {
+    if (!g || !plan3) return GIR_ERR_INVALID;
+    for (int i = 0; i < 3; ++i) plan3[i] = g->b_plan[i];
     return GIR_OK;
 }
 

@@ -126,6 +126,7 @@ struct gir_dev {
     // Batch statistics
     int64_t b_ins = 0, b_del = 0, b_noop = 0, b_invalid = 0;
     double b_ms[4] = {0, 0, 0, 0};    // phases of the last batch: store, WCC, SCC, BCT
+    int b_plan[3] = {2, 2, 2};        // what the last batch did per layer: 0 kept, 1 patched, 2 rebuilt
 
     // Schedule
     int schedule = GIR_SCHEDULE_FIXED;
@@ -237,7 +238,10 @@ int select_flagged_iota(gir_dev* g, const uint8_t* flags, int32_t* out, int64_t 
 // Components of the undirected view of a forward CSR; label = smallest vertex id (wcc.cu).
 int wcc_labels(gir_dev* g, const DevCSR& c, int32_t* label, int64_t* n_comp);
 int wcc_build(gir_dev* g);
+int wcc_union_pairs(gir_dev* g, const uint64_t* keys, int64_t n);
 int scc_build(gir_dev* g);
+// Condensation DAG and ranks from the current SCC labels (the labels are kept).
+int scc_build_dag(gir_dev* g);
 int bct_build(gir_dev* g);
 
 // ---- queries ----

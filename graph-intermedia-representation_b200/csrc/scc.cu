@@ -418,7 +418,12 @@ int scc_build(gir_dev* g) {
     GIR_TRY(ensure_n(g, g->scc, V + 1, &label));
     GIR_TRY(scc_labels(g, label, &g->n_scc));
     trace_mark(g, "scc: labels");
+    return scc_build_dag(g);
+}
 
+int scc_build_dag(gir_dev* g) {
+    const int64_t V = g->V;
+    int32_t* label = static_cast<int32_t*>(g->scc.p);
     // condensation edges: cross keys, radix sort, unique
     const int64_t cap = g->fw.cap;
     uint64_t *keys = nullptr, *tmp = nullptr;

@@ -50,6 +50,11 @@ __global__ void __launch_bounds__(kBlock) k_uf_link_rows(CSRView c, int64_t V, i
                     [&](int32_t u, int32_t w, int64_t) { uf_link(parent, u, w, err); });
 }
 
+// Links the endpoints of every pair key (u << 32 | v) into the existing forest.
+__global__ void k_uf_link_keys(const uint64_t* keys, int64_t n, int32_t* parent, int32_t* err) {
+    GRID_STRIDE(i, n) uf_link(parent, (int32_t)(keys[i] >> 32), (int32_t)(keys[i] & 0xffffffffULL), err);
+}
+
 // Final pointer jumping. The walk only reads: with path halving, another thread could replace
 // a root just stored in parent[v] by an intermediate ancestor; here every write is a final root.
 __global__ void k_uf_compress(int32_t* parent, int64_t V, unsigned long long* roots) {
@@ -85,6 +90,29 @@ int wcc_labels(gir_dev* g, const DevCSR& c, int32_t* label, int64_t* n_comp) {
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     if (h[1]) return fail(g, GIR_ERR_TIMEOUT, "wcc: union-find link exceeded its retry bound");
     *n_comp = (int64_t)h[0];
+    return GIR_OK;
+}
+
+// Inserted undirected pairs only (no pair disappeared): the current labels (smallest member,
+// so every label is its own root) are a union-find forest already; linking the new pairs into
+// it and flattening gives the labels a rebuild would give.
+int wcc_union_pairs(gir_dev* g, const uint64_t* keys, int64_t n) {
+    const int64_t V = g->V;
+    int32_t* label = static_cast<int32_t*>(g->wcc.p);
+    unsigned long long* roots = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[14], 4, &roots));
+    int32_t* err = reinterpret_cast<int32_t*>(roots + 1);
+    GIR_CUDA(g, cudaMemsetAsync(roots, 0, 2 * sizeof(unsigned long long), g->stream));
+    if (V == 0 || n == 0) return GIR_OK;
+    k_uf_link_keys<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(keys, n, label, err);
+    GIR_LAUNCH(g, "k_uf_link_keys");
+    k_uf_compress<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(label, V, roots);
+    GIR_LAUNCH(g, "k_uf_compress");
+    unsigned long long h[2] = {0, 0};
+    GIR_CUDA(g, cudaMemcpyAsync(h, roots, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    if (h[1]) return fail(g, GIR_ERR_TIMEOUT, "wcc: union-find link exceeded its retry bound");
+    g->n_wcc = (int64_t)h[0];
     return GIR_OK;
 }
 

@@ -184,6 +184,13 @@ class DeviceGraph:
         self._ck(dev_lib().gir_dev_batch_times(self._h, ptr(out)), "batch_times")
         return dict(zip(("store", "wcc", "scc", "bct"), out.tolist()))
 
+    def batch_plan(self):
+        """Per layer, what the last batch did: 'kept', 'patched' or 'rebuilt'."""
+        out = np.zeros(3, np.int32)
+        self._ck(dev_lib().gir_dev_batch_plan(self._h, ptr(out)), "batch_plan")
+        names = ("kept", "patched", "rebuilt")
+        return dict(zip(("wcc", "scc", "bct"), (names[i] for i in out.tolist())))
+
     def set_weight_rule(self, seed, lo, hi):
         self._ck(dev_lib().gir_dev_set_weight_rule(self._h, seed, lo, hi), "set_weight_rule")
 

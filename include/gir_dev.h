@@ -155,6 +155,13 @@ int gir_dev_apply_batch(gir_dev_t* g, const int32_t* u, const int32_t* v, const 
  * edge store, [1] WCC, [2] SCC + DAG + ranks, [3] blocks. */
 int gir_dev_batch_times(gir_dev_t* g, double* ms4);
 
+/* What the last apply_batch did to each built layer ([0] WCC, [1] SCC + DAG, [2] blocks):
+ * 0 kept (the batch cannot change it), 1 patched (WCC: inserted pairs unioned into the labels;
+ * SCC: labels kept, DAG and ranks rebuilt), 2 rebuilt. The reference repairs per update
+ * (handleInsert / deleteEdgeImpl, gir.cpp:3007-3131); here the decision is per batch, from exact
+ * sufficient conditions evaluated on the device. */
+int gir_dev_batch_plan(gir_dev_t* g, int32_t* plan3);
+
 /* Weight rule for edges inserted into a graph with stored weights (see apply_batch). */
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi);
 

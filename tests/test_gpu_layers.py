@@ -169,3 +169,58 @@ def test_shapes_high_diameter_and_dense(pkg, orc):
         fb, fa = orc.normalize(V, gg.fw_beg, gg.fw_adj)
         _oracle_match(pkg, orc, d, V, fb, fa, name)
         d.close()
+
+
+def test_batch_repair_plans_match_oracle(pkg, orc, s16):
+    """Small batches built to reach each repair decision (layers kept, WCC unioned, DAG-only SCC
+    refresh, full rebuilds), checked against the oracle after every batch; every decision the
+    batches are built for must be taken at least once."""
+    g, fb, fa = s16
+    V = g.V
+    d = pkg.DeviceGraph.from_graph(g)
+    d.build(pkg.native.LAYER_ALL)
+    rng = np.random.default_rng(77)
+    seen = {"wcc": set(), "scc": set(), "bct": set()}
+
+    def apply(u, v, ins, what):
+        nonlocal fb, fa
+        u = np.asarray(u, np.int32)
+        v = np.asarray(v, np.int32)
+        ins = np.asarray(ins, np.uint8)
+        d.apply_batch(u, v, ins)
+        for k, x in d.batch_plan().items():
+            seen[k].add(x)
+        fb, fa, _, _ = orc.apply_batch(V, fb, fa, u, v, ins)
+        _oracle_match(pkg, orc, d, V, fb, fa, what)
+
+    for step in range(4):
+        scc = d.labels(pkg.native.LABEL_SCC)
+        rank = d.labels(pkg.native.LABEL_SCC_RANK)
+        label, head = d.blocks()
+        # inserts inside one block of the giant SCC: every layer kept or WCC-unioned
+        big = np.bincount(scc).argmax()
+        members = np.nonzero(scc == big)[0]
+        blk = label[members]
+        b = np.bincount(blk).argmax()
+        inb = members[blk == b]
+        u, v = rng.choice(inb, 8), rng.choice(inb, 8)
+        keep = u != v
+        apply(u[keep], v[keep], np.ones(keep.sum()), f"same-block inserts {step}")
+        # inserts between SCCs that follow the rank order: labels kept, DAG refreshed
+        a, c = rng.integers(0, V, 64), rng.integers(0, V, 64)
+        fwd = (scc[a] != scc[c]) & (rank[a] < rank[c])
+        apply(a[fwd][:6], c[fwd][:6], np.ones(min(6, fwd.sum())), f"rank-forward inserts {step}")
+        # deletions of cross-SCC edges: labels kept, DAG refreshed
+        cb, ca = d.csr(0)
+        rows = np.repeat(np.arange(V), np.diff(cb))
+        cross = np.nonzero(scc[rows] != scc[ca])[0]
+        pick = rng.choice(cross, min(6, len(cross)), replace=False)
+        apply(rows[pick], ca[pick], np.zeros(len(pick)), f"cross deletions {step}")
+        # a random mixed batch (usually rebuilds)
+        gg = pkg.graphs.Graph(V, cb.astype(np.int32), ca, None, None)
+        u, v, ins = pkg.graphs.updates(gg, 20, 20, 300 + step)
+        apply(u, v, ins, f"random batch {step}")
+    d.close()
+    assert {"kept", "rebuilt"} <= seen["bct"], seen
+    assert {"kept", "patched", "rebuilt"} <= seen["scc"], seen
+    assert "patched" in seen["wcc"] or "kept" in seen["wcc"], seen

@@ -2,6 +2,7 @@
 // update pipeline, getters and query entry points.
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -802,6 +803,47 @@ int gir_dev_bfs(gir_dev_t* g, const int32_t* srcs, int64_t n_src, int32_t* level
     std::vector<int64_t> sb((size_t)n_src + 1);
     for (int64_t i = 0; i <= n_src; ++i) sb[i] = i;
     return query_sets(g, sb.data(), srcs, n_src, true, 0, 0, level_out);
+}
+
+int gir_dev_autotune(gir_dev_t* g, const int32_t* srcs, int64_t n_src, int reps, double* best_ms) {
+    if (!g) return GIR_ERR_INVALID;
+    if (n_src < 1 || n_src > 64 || !srcs || reps < 1)
+        return fail(g, GIR_ERR_INVALID, "autotune: need 1..64 sources and reps >= 1");
+    std::vector<int64_t> sb((size_t)n_src + 1);
+    for (int64_t i = 0; i <= n_src; ++i) sb[i] = i;
+    void* out = nullptr;
+    GIR_TRY(dev_alloc(g, &out, sizeof(int32_t) * (size_t)g->V * (size_t)n_src + 16));
+    const double keep[3] = {g->params[GIR_PARAM_CTAS_PER_SM], g->params[GIR_PARAM_SMALL_DEG],
+                            g->params[GIR_PARAM_LARGE_DEG]};
+    double best = 1e300, choice[3] = {keep[0], keep[1], keep[2]};
+    int rc = GIR_OK;
+    for (double ctas : {2.0, 4.0, 8.0})
+        for (double small : {8.0, 32.0, 128.0})
+            for (double large : {1024.0, 4096.0, 32768.0}) {
+                g->params[GIR_PARAM_CTAS_PER_SM] = ctas;
+                g->params[GIR_PARAM_SMALL_DEG] = small;
+                g->params[GIR_PARAM_LARGE_DEG] = large;
+                g->bins_valid = false;  // (the degree bins depend on the thresholds)
+                rc = query_sets(g, sb.data(), srcs, n_src, true, 0, 0, out);  // untimed: builds the bins
+                double t = 1e300;
+                for (int r = 0; rc == GIR_OK && r < reps; ++r) {
+                    rc = query_sets(g, sb.data(), srcs, n_src, true, 0, 0, out);
+                    t = std::min(t, g->qstats.total_ms);
+                }
+                if (rc != GIR_OK) break;
+                if (t < best) {
+                    best = t;
+                    choice[0] = ctas; choice[1] = small; choice[2] = large;
+                }
+            }
+    dev_free(g, out);
+    g->params[GIR_PARAM_CTAS_PER_SM] = rc == GIR_OK ? choice[0] : keep[0];
+    g->params[GIR_PARAM_SMALL_DEG] = rc == GIR_OK ? choice[1] : keep[1];
+    g->params[GIR_PARAM_LARGE_DEG] = rc == GIR_OK ? choice[2] : keep[2];
+    g->bins_valid = false;
+    if (rc != GIR_OK) return rc;
+    if (best_ms) *best_ms = best;
+    return GIR_OK;
 }
 
 int gir_dev_bfs_sets(gir_dev_t* g, const int64_t* set_beg, const int32_t* set_srcs, int64_t n_sets, int32_t* level_out) {

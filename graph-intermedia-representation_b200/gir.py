@@ -184,6 +184,16 @@ class DeviceGraph:
         self._ck(dev_lib().gir_dev_batch_times(self._h, ptr(out)), "batch_times")
         return dict(zip(("store", "wcc", "scc", "bct"), out.tolist()))
 
+    def autotune(self, sources, reps=2):
+        """Picks the grid size and degree-bin thresholds by timing BFS from `sources` (1..64);
+        returns the chosen parameters and the winner's ms per call."""
+        s, n = self._ids(sources)
+        best = ctypes.c_double()
+        self._ck(dev_lib().gir_dev_autotune(self._h, ptr(s), n, int(reps), ctypes.byref(best)), "autotune")
+        P = native
+        return {"ctas_per_sm": self.get_param(P.PARAM_CTAS_PER_SM), "small_deg": self.get_param(P.PARAM_SMALL_DEG),
+                "large_deg": self.get_param(P.PARAM_LARGE_DEG), "bfs_ms": best.value}
+
     def batch_plan(self):
         """Per layer, what the last batch did: 'kept', 'patched' or 'rebuilt'."""
         out = np.zeros(3, np.int32)

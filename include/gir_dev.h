@@ -162,6 +162,14 @@ int gir_dev_batch_times(gir_dev_t* g, double* ms4);
  * sufficient conditions evaluated on the device. */
 int gir_dev_batch_plan(gir_dev_t* g, int32_t* plan3);
 
+/* Autotuner (no counterpart in the reference, whose OpenMP loops take no launch shapes): times
+ * gir_dev_bfs on `srcs` (1..64 sources, host or device) for every combination of
+ * GIR_PARAM_CTAS_PER_SM in {2, 4, 8}, GIR_PARAM_SMALL_DEG in {8, 32, 128} and GIR_PARAM_LARGE_DEG
+ * in {1024, 4096, 32768}, best of `reps` calls each, and keeps the fastest setting on the handle
+ * (read it back with gir_dev_get_param). The parameters shape launches only, so results never
+ * change. *best_ms (may be NULL) = the winner's device time per call. */
+int gir_dev_autotune(gir_dev_t* g, const int32_t* srcs, int64_t n_src, int reps, double* best_ms);
+
 /* Weight rule for edges inserted into a graph with stored weights (see apply_batch). */
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi);
 
@@ -182,7 +190,7 @@ enum {
     GIR_PARAM_ALPHA = 0,        /* top-down -> bottom-up when frontier edges * alpha > unexplored */
     GIR_PARAM_BETA = 1,         /* bottom-up -> top-down when frontier * beta < vertices */
     GIR_PARAM_DELTA = 2,        /* default Delta of the fixed schedule */
-    GIR_PARAM_BLOCK = 3,        /* threads per CTA of the traversal kernels */
+    GIR_PARAM_BLOCK = 3,        /* accepted and stored; the kernels use fixed 256-thread CTAs */
     GIR_PARAM_SMALL_DEG = 4,    /* degree bin: thread per vertex below this in-degree */
     GIR_PARAM_LARGE_DEG = 5,    /* degree bin: CTA per vertex from this in-degree on */
     GIR_PARAM_CTAS_PER_SM = 6,  /* grid size = SMs x this */

@@ -222,3 +222,17 @@ def test_has_edges(pkg, s16):
     assert d.has_edges(fa[pick], rows[pick], undirected=True).all()
     assert not d.has_edges([0, -1, g.V], [0, 1, 2]).any()
     d.close()
+
+
+def test_autotune_keeps_results(pkg, s16):
+    g, _, _ = s16
+    d = pkg.DeviceGraph.from_graph(g)
+    src = pkg.graphs.sources_with_edges(g, 32, 44)
+    before = d.bfs(src)
+    res = d.autotune(src, reps=1)
+    assert res["ctas_per_sm"] in (2, 4, 8) and res["small_deg"] in (8, 32, 128)
+    assert res["large_deg"] in (1024, 4096, 32768) and res["bfs_ms"] > 0
+    np.testing.assert_array_equal(d.bfs(src), before)
+    with pytest.raises(pkg.GirError):
+        d.autotune(np.zeros(65, np.int32))
+    d.close()

@@ -450,13 +450,21 @@ def run_ours(args):
                   "scc_dag_ms": ev_time(stream, lambda: d.build(native.LAYER_SCC)),
                   "bct_ms": ev_time(stream, lambda: d.build(native.LAYER_BCT))}
         extra["build"] = builds
+        rep = None
+        if world > 1:  # replicas: rank 0's batch is broadcast, so every replica stays identical
+            rep = importlib.import_module("graph-intermedia-representation_b200.replicas").Replicas(d)
         for n in (10_000, 100_000, 1_000_000):
-            u, v, ins = pkg.graphs.updates(g, n // 2, n // 2, 50 + n + rank)
+            if rep is not None:
+                u, v, ins = rep.broadcast_batch(*(pkg.graphs.updates(g, n // 2, n // 2, 50 + n) if rank == 0 else ()))
+            else:
+                u, v, ins = pkg.graphs.updates(g, n // 2, n // 2, 50 + n)
             ub, vb, ib = (torch.from_numpy(x).pin_memory() for x in (u, v, ins))
             t = ev_time(stream, lambda: d.apply_batch(ub.numpy(), vb.numpy(), ib.numpy()))
             upd[str(n)] = n / (t * 1e-3)
             extra.setdefault("update_phases_ms", {})[str(n)] = {k: round(x, 2) for k, x in d.batch_times().items()}
         extra["updates_per_s"] = upd
+        if rep is not None:
+            extra["replicas_agree_checksum"] = rep.check_agree()
 
     # batched source sets interleaved with uneven update batches (on the updated graph)
     if not args.no_batched and not args.no_updates:

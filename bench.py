@@ -53,6 +53,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-schedule", action="store_true", help="skip the learned-vs-fixed schedule comparison")
     p.add_argument("--no-batched", action="store_true", help="skip the batched queries + uneven batches section")
+    p.add_argument("--stream", type=int, default=0, metavar="ROUNDS",
+                   help="instead of the bench: the 41.6M-vertex / 1.47B-edge R-MAT (seed 5, weights U[1,1023]), "
+                        "WCC + SCC build, then ROUNDS x (1M-edge batch 60/40 + 32 BFS + 32 SSSP), checked by "
+                        "the size-independent certificates; one JSON line")
     p.add_argument("--only", choices=["bfs", "sssp", "build"], default=None,
                    help="profiling runs: one call of one query kind (or the three layer builds and one "
                         "10K update batch), no timing and no JSON line")
@@ -333,6 +337,52 @@ def batched_section(pkg, d, g, stream, dev, rounds=64, seed=90):
                     "weights), every layer kept exact after every batch"}
 
 
+def run_stream(args):
+    """The large power-law configuration as a stream (see --stream)."""
+    import numpy as np
+    import torch
+    pkg = importlib.import_module("graph-intermedia-representation_b200")
+    vf = importlib.import_module("graph-intermedia-representation_b200.verify")
+    native = pkg.native
+    t0 = time.time()
+    g = pkg.graphs.rmat_tw()
+    t_gen = time.time() - t0
+    d = pkg.DeviceGraph.from_graph(g)
+    stream = torch.cuda.ExternalStream(d.stream(), device="cuda:0")
+    t_create = time.time() - t0 - t_gen
+    builds = {"wcc_ms": ev_time(stream, lambda: d.build(native.LAYER_WCC)),
+              "scc_dag_ms": ev_time(stream, lambda: d.build(native.LAYER_SCC))}
+    lv = torch.empty((32, g.V), dtype=torch.int32, device="cuda:0")
+    ds = torch.empty((32, g.V), dtype=torch.int64, device="cuda:0")
+    rows = []
+    for r in range(args.stream):
+        u, v, ins = pkg.graphs.updates(g, 600_000, 400_000, 500 + r)
+        t_b = ev_time(stream, lambda: d.apply_batch(u, v, ins))
+        src = torch.from_numpy(pkg.graphs.sources_with_edges(g, 32, 600 + r)).to("cuda:0")
+        t_q = ev_time(stream, lambda: d.bfs(src, out=lv))
+        e_b = d.query_stats()["edges"]
+        t_s = ev_time(stream, lambda: d.sssp(src, delta=0 if r % 2 else 16, weights=native.WEIGHT_STORED, out=ds))
+        e_s = d.query_stats()["edges"]
+        rows.append({"batch_ms": t_b, "bfs_ms": t_q, "bfs_gteps": e_b / (t_q * 1e-3) / 1e9, "sssp_ms": t_s,
+                     "sssp_gteps": e_s / (t_s * 1e-3) / 1e9, "sssp_schedule": "learned" if r % 2 else "fixed",
+                     "plan": d.batch_plan()})
+        if r == 0:
+            d.use_learned_schedule()
+    fb, fa = d.csr(0)
+    s_last = src.cpu().numpy()
+    cert = {"bfs": vf.bfs_levels(fb, fa, [s_last[0]], lv[0]), "wcc": vf.wcc_labels(fb, fa, d.labels(native.LABEL_WCC))}
+    s_d, t_d = d.dag()
+    cert["scc_dag"] = vf.scc_dag(fb, fa, d.labels(native.LABEL_SCC), d.labels(native.LABEL_SCC_RANK), s_d, t_d)
+    d.sssp(src[:1], delta=0, weights=native.WEIGHT_HASH, out=ds[:1])
+    cert["sssp_hash"] = vf.sssp_dists(fb, fa, [s_last[0]], ds[0])
+    c = d.counts()
+    print(json.dumps({"stream": "rmat_tw", "V": c["V"], "E": c["E"], "n_scc": c["n_scc"], "n_wcc": c["n_wcc"],
+                      "generate_s": t_gen, "create_s": t_create, "build": builds, "rounds": rows,
+                      "updates_per_s": 1e6 * len(rows) / (1e-3 * sum(x["batch_ms"] for x in rows)),
+                      "certificate_violations": cert}), flush=True)
+    d.close()
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -516,6 +566,8 @@ def main():
     args = parse()
     if args.only:
         run_only(args)
+    elif args.stream:
+        run_stream(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -578,6 +578,7 @@ int query_sets(gir_dev* g, const int64_t* set_beg_user, const int32_t* srcs, int
     float ms = 0;
     GIR_CUDA(g, cudaEventElapsedTime(&ms, t0, t1));
     g->qstats.total_ms = ms;
+    release_scratch(g, kKeepScratchBelow);
     return GIR_OK;
 }
 
@@ -588,7 +589,7 @@ double now_ms() {
 }
 
 void trace_mark(gir_dev* g, const char* what) {
-    if (!g->trace_on) return;
+    if (!g->trace_marks) return;
     cudaStreamSynchronize(g->stream);
     const double t = now_ms();
     std::fprintf(stderr, "[gir] %-28s %9.3f ms\n", what, g->trace_t > 0 ? t - g->trace_t : 0.0);
@@ -703,6 +704,7 @@ int gir_dev_build(gir_dev_t* g, unsigned layers) {
         if (!g->scc_built) return fail(g, GIR_ERR_STATE, "buildBCT needs buildSCC_DAG first (gir.h:98)");
         GIR_TRY(bct_build(g));
     }
+    release_scratch(g, kKeepScratchBelow);
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     return GIR_OK;
 }
@@ -866,7 +868,9 @@ int gir_dev_sssp_sets(gir_dev_t* g, const int64_t* set_beg, const int32_t* set_s
 int gir_dev_apply_batch(gir_dev_t* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n) {
     if (!g) return GIR_ERR_INVALID;
     if (n < 0 || (n > 0 && (!u || !v || !ins))) return fail(g, GIR_ERR_INVALID, "apply_batch: bad arguments");
-    return apply_batch_impl(g, u, v, ins, n);
+    const int rc = apply_batch_impl(g, u, v, ins, n);
+    release_scratch(g, kKeepScratchBelow);
+    return rc;
 }
 
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi) {

@@ -143,8 +143,10 @@ struct gir_dev {
     double wstat[2][2] = {{0, 0}, {0, 0}};  // per weight mode: mean and max weight (set with ws)
     std::string err;
     // Phase trace on stderr (environment GIR_TRACE=1): each mark synchronizes and prints the
-    // wall time since the previous one, and every scratch allocation is reported.
+    // wall time since the previous one, and every scratch allocation is reported; GIR_TRACE=2
+    // reports the allocations only (no synchronizing marks).
     bool trace_on = std::getenv("GIR_TRACE") != nullptr;
+    bool trace_marks = trace_on && std::string(std::getenv("GIR_TRACE")) != "2";
     double trace_t = 0;
 };
 
@@ -181,6 +183,11 @@ int ensure_n(gir_dev* g, DevBuf& b, size_t n, T** out) {
     return GIR_OK;
 }
 void release(gir_dev* g, DevBuf& b);
+// Returns every working buffer of at least `min_bytes` to the handle's pool (top-level calls do
+// this on return: the pool hands the memory to the next phase that needs it, so the phases share
+// one working set instead of each keeping its own high-water mark).
+void release_scratch(gir_dev* g, size_t min_bytes);
+constexpr size_t kKeepScratchBelow = 64u << 20;
 
 // Pinned host scratch of at least `bytes`.
 int pinned(gir_dev* g, size_t bytes, void** out);

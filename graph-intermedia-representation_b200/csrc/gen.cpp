@@ -87,15 +87,17 @@ int gir_gen_rmat(int scale, int64_t V, int64_t n_draws, int64_t target_unique, d
     uint64_t want = (uint64_t)(target_unique > 0 ? (double)target_unique * 1.3 + 1024 : (double)n_draws);
     for (int attempt = 0; attempt < 8; ++attempt) {
         const uint64_t lo = drawn, hi = want;
-        std::vector<Draw> add(hi - lo);
-        #pragma omp parallel for schedule(static)
-        for (int64_t i = (int64_t)lo; i < (int64_t)hi; ++i) {
-            uint64_t u, v;
-            rmatDraw(seed, (uint64_t)i, scale, a, b, c, u, v);
-            add[i - lo] = (u == v || u >= (uint64_t)V || v >= (uint64_t)V) ? Draw{~0ULL, (uint64_t)i}
-                                                                           : Draw{(u << 32) | v, (uint64_t)i};
+        {  // (the new draws are released before the sort: peak memory is the sort's, not 3x)
+            std::vector<Draw> add(hi - lo);
+            #pragma omp parallel for schedule(static)
+            for (int64_t i = (int64_t)lo; i < (int64_t)hi; ++i) {
+                uint64_t u, v;
+                rmatDraw(seed, (uint64_t)i, scale, a, b, c, u, v);
+                add[i - lo] = (u == v || u >= (uint64_t)V || v >= (uint64_t)V) ? Draw{~0ULL, (uint64_t)i}
+                                                                               : Draw{(u << 32) | v, (uint64_t)i};
+            }
+            d.insert(d.end(), add.begin(), add.end());
         }
-        d.insert(d.end(), add.begin(), add.end());
         drawn = hi;
         psort(d);
         size_t m = 0;

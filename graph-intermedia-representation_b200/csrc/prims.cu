@@ -23,7 +23,19 @@ int cuda_check(gir_dev* g, cudaError_t e, const char* what) {
 int dev_alloc(gir_dev* g, void** p, size_t bytes) {
     *p = nullptr;
     const size_t want = ((bytes < 256 ? 256 : bytes) + 255) & ~(size_t)255;
-    const cudaError_t e = cudaMallocFromPoolAsync(p, want, g->pool, g->stream);
+    const double t0 = g->trace_on ? now_ms() : 0.0;
+    cudaError_t e = cudaMallocFromPoolAsync(p, want, g->pool, g->stream);
+    if (e == cudaErrorMemoryAllocation) {
+        if (g->trace_on) std::fprintf(stderr, "[gir] pool exhausted at %zu bytes: trimming\n", want);
+        // The pool keeps freed blocks for reuse; when none fits, give its unused memory back to
+        // the device and try once more (large graphs use most of HBM in turns).
+        cudaGetLastError();
+        cudaStreamSynchronize(g->stream);
+        cudaMemPoolTrimTo(g->pool, 0);
+        e = cudaMallocFromPoolAsync(p, want, g->pool, g->stream);
+    }
+    if (g->trace_on && now_ms() - t0 > 1.0)
+        std::fprintf(stderr, "[gir] pool allocation of %zu bytes took %.3f ms\n", want, now_ms() - t0);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -49,6 +61,19 @@ int ensure(gir_dev* g, DevBuf& b, size_t bytes) {
     if (g->trace_on) std::fprintf(stderr, "[gir] alloc %zu bytes: %.3f ms\n", want, now_ms() - t0);
     b.bytes = want;
     return GIR_OK;
+}
+
+void release_scratch(gir_dev* g, size_t min_bytes) {
+    auto drop = [&](DevBuf& b) {
+        if (b.p && b.bytes >= min_bytes) release(g, b);
+    };
+    for (auto& b : g->scratch) drop(b);
+    for (auto& b : g->work) drop(b);
+    for (auto& b : g->qitems) drop(b);
+    drop(g->cub_tmp);
+    drop(g->stage_in);
+    drop(g->stage_out);
+    drop(g->lane_dist);
 }
 
 void release(gir_dev* g, DevBuf& b) {

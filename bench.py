@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="rmat_lj", choices=["rmat_lj", "rmat_s20", "rmat_s16"])
+    p.add_argument("--workload", default="rmat_lj", choices=["rmat_lj", "rmat_s20", "rmat_s16", "lattice_2000"])
     p.add_argument("--no-updates", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-schedule", action="store_true", help="skip the learned-vs-fixed schedule comparison")
@@ -68,6 +68,8 @@ def workload(pkg, name):
         return pkg.graphs.rmat_lj()
     if name == "rmat_s20":  # 1M vertices, 2^24 draws: a profiling case larger than L2
         return pkg.graphs.rmat(20, seed=3, permute=True, name="rmat_s20")
+    if name == "lattice_2000":  # 4M vertices, the lattice procedure at side 2000: a profiling case
+        return pkg.graphs.lattice(side=2000)
     return pkg.graphs.rmat_s16()
 
 

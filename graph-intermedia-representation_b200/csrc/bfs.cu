@@ -13,7 +13,11 @@
 //  - bottom-up: every vertex that some lane has not reached ORs its in-neighbours' frontier
 //    masks and stops once every missing lane is found (gir_query.cpp:232-279), with vertices
 //    binned by in-degree: a thread, a warp or a CTA per vertex.
+#include <algorithm>
+#include <cstring>
+
 #include "common.cuh"
+#include "sched_net.cuh"
 
 namespace gir {
 
@@ -61,6 +65,258 @@ __global__ void k_init_sources(const int64_t* set_beg, int n_lanes, const int32_
     }
 }
 
+// ---- Persistent top-down levels ----------------------------------------------------------------
+// A high-diameter graph (a road network, a lattice) takes thousands of levels whose frontiers are
+// small: driven from the host, every level costs launches and a synchronization. While the
+// frontier stays small and the schedule stays top-down, one cooperative launch runs level after
+// level instead, its CTAs meeting at a grid barrier between the expand and the commit phase. It
+// hands back to the host loop when the schedule turns bottom-up, when the frontier's out-edges or
+// a frontier vertex's degree outgrow what warps walking whole rows balance well, or when done.
+// Data that other CTAs write during the launch (masks, queues, counters) is read with ld.cg, past
+// the SMs' incoherent L1; every barrier wait is bounded and sets an error flag when it runs out.
+constexpr int kPersistThreads = 256;
+constexpr int64_t kPersistMaxEdges = 1ll << 28;  // a frontier's out-edges (vertex level)
+constexpr int kPersistMaxDeg = 4096;              // a frontier vertex's out-degree
+constexpr int kPersistTrace = 8192;               // schedule decisions recorded per launch
+constexpr unsigned kBarrierSpins = 1u << 25;      // bounded barrier wait (a few seconds)
+
+// control words; counter slots (one per level, reused every third level) follow
+enum { P_LEVELS = 0, P_NQ, P_REASON, P_DIR, P_EDGES, P_REACHED, P_MF, P_NF, P_MU, P_FI, P_QI, P_ERR, P_SLOTS = 16 };
+enum { S_Q = 0, S_CAND, S_PAIRS, S_MEDGES, S_VEDGES, S_MAXDEG, S_W = 8 };
+enum { R_DONE = 0, R_BOTTOM_UP = 1, R_BIG = 2, R_LIMIT = 3 };
+// the barrier's arrival counter and generation, each on its own 128-byte line after the slots
+constexpr int kCtlBarrier = 64;
+constexpr int kCtlWords = kCtlBarrier + 32;
+
+struct PersistArgs {
+    CSRView fw;
+    uint64_t* seen;
+    uint64_t* next;
+    uint64_t* front[2];       // the frontier's masks alternate between these (the other is zero)
+    int32_t* q[3];            // frontier, candidates and next frontier rotate over these
+    int32_t* level;
+    int64_t V, nq0;
+    double E, mf0, nf0, mu0, alpha, beta;
+    int lanes, L0, max_levels;
+    const float* net;         // schedule network parameters, or null for the fixed switch
+    unsigned long long* ctl;  // P_* words and the counter slots, zeroed by the host
+    unsigned int* bar;        // [0] arrivals, [32] generation (own 128-byte lines), zeroed by the host
+    float* trace;             // kPersistTrace x (GIR_SCHED_IN features + decision)
+};
+
+__device__ __forceinline__ unsigned long long ldcg_u64(const unsigned long long* p) { return __ldcg(p); }
+
+// All CTAs of the cooperative launch meet here. Returns false once any CTA has flagged an error.
+__device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned long long* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = bar + 32;
+        const unsigned int g0 = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 32, 1u);
+        } else {
+            unsigned int spins = 0;
+            while (*gen == g0) {
+                if (++spins > kBarrierSpins) {
+                    atomicExch(err, 1ull);
+                    break;
+                }
+                if ((spins & 63) == 0 && ldcg_u64(err) != 0ull) break;
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ldcg_u64(err) == 0ull;
+}
+
+// End of a phase: the CTA's warps empty their staging buffers with one queue reservation for the
+// whole CTA (block-uniform call; s_cnt holds one int per warp, s_base one word).
+__device__ __forceinline__ void block_flush(int32_t* s_buf, int& s_n, int* s_cnt, unsigned long long* s_base, int32_t* q,
+                                            unsigned long long* cnt) {
+    const int wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane_id() == 0) s_cnt[wib] = s_n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int total = 0;
+        for (int k = 0; k < nw; ++k) total += s_cnt[k];
+        *s_base = total ? atomicAdd(cnt, (unsigned long long)total) : 0ull;
+    }
+    __syncthreads();
+    unsigned long long off = *s_base;
+    for (int k = 0; k < wib; ++k) off += s_cnt[k];
+    for (int i = lane_id(); i < s_n; i += 32) q[off + i] = s_buf[i];
+    s_n = 0;
+    __syncthreads();
+}
+
+// Sums v over the CTA (block-uniform call) and adds it to *dst with one atomic per CTA; with
+// max_ set, takes the maximum instead.
+__device__ __forceinline__ void block_add(unsigned long long v, unsigned long long* s_red, unsigned long long* dst,
+                                          bool max_) {
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = max_ ? (t > v ? t : v) : v + t;
+    }
+    if (lane_id() == 0) s_red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long r = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = max_ ? (s_red[k] > r ? s_red[k] : r) : r + s_red[k];
+        if (r) {
+            if (max_) atomicMax(dst, r);
+            else atomicAdd(dst, r);
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPersistThreads) k_bfs_persistent(PersistArgs a) {
+    __shared__ int64_t s_excl[kPersistThreads / 32][33];
+    __shared__ int32_t s_u[kPersistThreads / 32][32];
+    __shared__ int s_dir;
+    __shared__ int32_t s_stage[kPersistThreads / 32][kStage];
+    __shared__ int s_cnt[kPersistThreads / 32];
+    __shared__ unsigned long long s_red[kPersistThreads / 32];
+    __shared__ unsigned long long s_base;
+    unsigned long long* err = a.ctl + P_ERR;
+    const int lane = lane_id(), wib = threadIdx.x >> 5;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    int fi = 0, qi = 0, reason = R_LIMIT, dir = 0, lev = 0, n_st = 0;
+    int64_t nq = a.nq0, vedges = 0, maxdeg = 0;
+    double mf = a.mf0, nf = a.nf0, mu = a.mu0;
+    unsigned long long edges = 0, reached = 0;
+    for (lev = 0; lev < a.max_levels; ++lev) {
+        if (threadIdx.x == 0) {  // (every CTA computes the same decision from the same counters)
+            float x[sched_net::IN];
+            s_dir = sched_net::decide_direction(a.net, (double)a.V, a.E, nf, mf, mu, 0, a.lanes, a.alpha, a.beta, x);
+            if (blockIdx.x == 0 && lev < kPersistTrace) {
+                for (int i = 0; i < sched_net::IN; ++i) a.trace[lev * (sched_net::IN + 1) + i] = x[i];
+                a.trace[lev * (sched_net::IN + 1) + sched_net::IN] = (float)s_dir;
+            }
+        }
+        __syncthreads();
+        dir = s_dir;
+        __syncthreads();  // (s_dir is rewritten at the next level only after every thread read it)
+        if (dir) { reason = R_BOTTOM_UP; break; }
+        if (lev > 0 && (vedges > kPersistMaxEdges || maxdeg > kPersistMaxDeg)) { reason = R_BIG; break; }
+        unsigned long long* sl = a.ctl + P_SLOTS + S_W * (lev % 3);
+        unsigned long long* sl_done = a.ctl + P_SLOTS + S_W * ((lev + 2) % 3);  // last level's slot
+        const int32_t* qa = a.q[qi];
+        int32_t* qb = a.q[(qi + 1) % 3];
+        int32_t* qc = a.q[(qi + 2) % 3];
+        uint64_t* fA = a.front[fi];
+        uint64_t* fB = a.front[fi ^ 1];
+        // expand: a warp takes 32 frontier vertices and walks their rows together; a lane bit that
+        // newly reaches w goes into next[w], and the atomicOr that turns next[w] non-zero queues w
+        for (int64_t base = warp * 32; base < nq; base += nwarps * 32) {
+            const int64_t i = base + lane;
+            const int32_t u = i < nq ? __ldcg(qa + i) : -1;
+            const int64_t cnt = u >= 0 ? a.fw.deg[u] : 0;
+            int64_t incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            s_excl[wib][lane] = incl - cnt;
+            if (lane == 31) s_excl[wib][32] = incl;
+            s_u[wib][lane] = u;
+            __syncwarp();
+            const int64_t total = s_excl[wib][32];
+            for (int64_t p0 = 0; p0 < total; p0 += 32) {
+                const int64_t p = p0 + lane;
+                bool fresh = false;
+                int32_t w = 0;
+                if (p < total) {
+                    int lo = 0, hi = 31;
+                    while (lo < hi) {
+                        const int m = (lo + hi + 1) >> 1;
+                        if (s_excl[wib][m] <= p) lo = m; else hi = m - 1;
+                    }
+                    const int32_t uu = s_u[wib][lo];
+                    w = a.fw.adj[a.fw.beg[uu] + (p - s_excl[wib][lo])];
+                    const unsigned long long bits =
+                        ldcg_u64((const unsigned long long*)fA + uu) & ~ldcg_u64((const unsigned long long*)a.seen + w);
+                    if (bits) fresh = atomicOr((unsigned long long*)a.next + w, bits) == 0ull;
+                }
+                stage_append(fresh, w, s_stage[wib], n_st, qb, &sl[S_CAND]);
+            }
+            __syncwarp();
+        }
+        block_flush(s_stage[wib], n_st, s_cnt, &s_base, qb, &sl[S_CAND]);
+        if (!grid_sync(a.bar, err)) break;
+        // commit: clear the old frontier's masks, then every candidate takes its new lanes
+        if (blockIdx.x == 0 && threadIdx.x < S_W) sl_done[threadIdx.x] = 0;  // (read by every CTA before the barrier)
+        GRID_STRIDE(i, nq) fA[__ldcg(qa + i)] = 0;
+        const int64_t nc = (int64_t)ldcg_u64(&sl[S_CAND]);
+        unsigned long long pairs = 0, medges = 0, ved = 0, mdeg = 0;
+        for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nc; base += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t i = base + threadIdx.x;
+            bool on = false;
+            int32_t w = 0;
+            if (i < nc) {
+                w = __ldcg(qb + i);
+                const unsigned long long sw = ldcg_u64((const unsigned long long*)a.seen + w);
+                const unsigned long long nb = ldcg_u64((const unsigned long long*)a.next + w) & ~sw;
+                a.next[w] = 0;
+                if (nb) {
+                    a.seen[w] = sw | nb;
+                    fB[w] = nb;
+                    write_levels(a.level, a.V, w, nb, a.L0 + lev + 1);
+                    const unsigned c = __popcll(nb);
+                    const unsigned long long d = (unsigned long long)a.fw.deg[w];
+                    pairs += c;
+                    medges += c * d;
+                    ved += d;
+                    mdeg = d > mdeg ? d : mdeg;
+                    on = true;
+                }
+            }
+            stage_append(on, w, s_stage[wib], n_st, qc, &sl[S_Q]);
+        }
+        block_flush(s_stage[wib], n_st, s_cnt, &s_base, qc, &sl[S_Q]);
+        block_add(pairs, s_red, &sl[S_PAIRS], false);
+        block_add(medges, s_red, &sl[S_MEDGES], false);
+        block_add(ved, s_red, &sl[S_VEDGES], false);
+        block_add(mdeg, s_red, &sl[S_MAXDEG], true);
+        if (!grid_sync(a.bar, err)) break;
+        nq = (int64_t)ldcg_u64(&sl[S_Q]);
+        const unsigned long long pr = ldcg_u64(&sl[S_PAIRS]), me = ldcg_u64(&sl[S_MEDGES]);
+        vedges = (int64_t)ldcg_u64(&sl[S_VEDGES]);
+        maxdeg = (int64_t)ldcg_u64(&sl[S_MAXDEG]);
+        nf = (double)pr / a.lanes;
+        mf = (double)me / a.lanes;
+        mu -= mf;
+        edges += me;
+        reached += pr;
+        fi ^= 1;
+        qi = (qi + 2) % 3;
+        if (nq == 0) {
+            reason = R_DONE;
+            ++lev;
+            break;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.ctl[P_LEVELS] = (unsigned long long)lev;
+        a.ctl[P_NQ] = (unsigned long long)nq;
+        a.ctl[P_REASON] = (unsigned long long)reason;
+        a.ctl[P_DIR] = (unsigned long long)dir;
+        a.ctl[P_EDGES] = edges;
+        a.ctl[P_REACHED] = reached;
+        a.ctl[P_MF] = (unsigned long long)__double_as_longlong(mf);
+        a.ctl[P_NF] = (unsigned long long)__double_as_longlong(nf);
+        a.ctl[P_MU] = (unsigned long long)__double_as_longlong(mu);
+        a.ctl[P_FI] = (unsigned long long)fi;
+        a.ctl[P_QI] = (unsigned long long)qi;
+    }
+}
+
 // Frontier out-degrees for the edge-balanced expand.
 __global__ void k_frontier_degrees(const int32_t* q, int64_t nq, const int32_t* deg, int64_t* pref) {
     GRID_STRIDE(i, nq) pref[i] = deg[q[i]];
@@ -73,6 +329,8 @@ __global__ void k_td_expand(const int32_t* q, int64_t nq, const int64_t* pref, C
                             const uint64_t* front, const uint64_t* seen, uint64_t* next, int32_t* cand,
                             unsigned long long* cnt) {
     const int64_t total = pref[nq];  // (read here, so the host needs no copy of it)
+    __shared__ int32_t s_stage[kBlock / 32][kStage];
+    int n_st = 0;
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -97,9 +355,10 @@ __global__ void k_td_expand(const int32_t* q, int64_t nq, const int64_t* pref, C
                 const uint64_t bits = front[u] & ~seen[w];
                 if (bits) fresh = atomicOr((unsigned long long*)&next[w], (unsigned long long)bits) == 0ull;
             }
-            warp_append(fresh, w, cand, &cnt[C_CAND]);
+            stage_append(fresh, w, s_stage[threadIdx.x >> 5], n_st, cand, &cnt[C_CAND]);
         }
     }
+    stage_flush(s_stage[threadIdx.x >> 5], n_st, cand, &cnt[C_CAND]);
 }
 
 __global__ void k_clear_front(const int32_t* q, int64_t nq, uint64_t* front) {
@@ -111,6 +370,8 @@ __global__ void k_td_commit(const unsigned long long* n_cand, const int32_t* can
                             uint64_t* next, const int32_t* outdeg, int32_t* level, int64_t V, int32_t L, int32_t* q,
                             unsigned long long* cnt) {
     const int64_t nc = (int64_t)*n_cand;
+    __shared__ int32_t s_stage[kBlock / 32][kStage];
+    int n_st = 0;
     unsigned long long pairs = 0, medges = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nc; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
@@ -131,8 +392,9 @@ __global__ void k_td_commit(const unsigned long long* n_cand, const int32_t* can
                 on = true;
             }
         }
-        warp_append(on, w, q, &cnt[C_Q]);
+        stage_append(on, w, s_stage[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
     }
+    stage_flush(s_stage[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
     warp_add_u64(&cnt[C_PAIRS], pairs);
     warp_add_u64(&cnt[C_MEDGES], medges);
 }
@@ -141,6 +403,8 @@ __global__ void k_td_commit(const unsigned long long* n_cand, const int32_t* can
 __global__ void k_bu_thread(const int32_t* ids, int64_t n, CSRView bw, const uint64_t* front, uint64_t* seen,
                             uint64_t* next, uint64_t all, const int32_t* outdeg, int32_t* level, int64_t V,
                             int32_t L, int32_t* q, unsigned long long* cnt) {
+    __shared__ int32_t s_stage[kBlock / 32][kStage];
+    int n_st = 0;
     unsigned long long pairs = 0, medges = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
@@ -170,8 +434,9 @@ __global__ void k_bu_thread(const int32_t* ids, int64_t n, CSRView bw, const uin
                 on = true;
             }
         }
-        warp_append(on, v, q, &cnt[C_Q]);
+        stage_append(on, v, s_stage[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
     }
+    stage_flush(s_stage[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
     warp_add_u64(&cnt[C_PAIRS], pairs);
     warp_add_u64(&cnt[C_MEDGES], medges);
 }
@@ -321,6 +586,27 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
     const double alpha = g->params[GIR_PARAM_ALPHA], beta = g->params[GIR_PARAM_BETA];
     const int64_t E = g->fw.E;
     const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
+    // persistent top-down levels (graphs of 4096+ vertices; the device must take cooperative launches)
+    uint64_t* front2 = nullptr;
+    int32_t* q3 = nullptr;
+    unsigned long long* pctl = nullptr;
+    float* ptrace = nullptr;
+    int persist_grid = 0;
+    if (V >= 4096) {
+        int coop = 0, per_sm = 0;
+        GIR_CUDA(g, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g->device));
+        GIR_CUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_persistent, kPersistThreads, 0));
+        if (coop && per_sm > 0) {
+            persist_grid = g->num_sms * per_sm;  // every co-resident CTA: the levels are latency-bound
+            GIR_TRY(ensure_n(g, g->scratch[8], V, &front2));
+            GIR_TRY(ensure_n(g, g->scratch[9], V + 1, &q3));
+            GIR_TRY(ensure_n(g, g->scratch[10], kCtlWords, &pctl));
+            GIR_TRY(ensure_n(g, g->scratch[11], (size_t)kPersistTrace * (GIR_SCHED_IN + 1), &ptrace));
+        }
+    }
+    const float* net = nullptr;
+    if (g->schedule == GIR_SCHEDULE_LEARNED && g->sched_loaded) net = static_cast<const float*>(g->sched_w.p);
+    std::vector<float> trace_rows;
     MainTimer timer{g, g->params[GIR_PARAM_PROFILE] != 0.0};
     GIR_CUDA(g, cudaEventRecord(g->ev0, g->stream));
 
@@ -331,6 +617,7 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
         GIR_CUDA(g, cudaMemsetAsync(seen, 0, sizeof(uint64_t) * V, g->stream));
         GIR_CUDA(g, cudaMemsetAsync(front, 0, sizeof(uint64_t) * V, g->stream));
         GIR_CUDA(g, cudaMemsetAsync(next, 0, sizeof(uint64_t) * V, g->stream));
+        if (front2) GIR_CUDA(g, cudaMemsetAsync(front2, 0, sizeof(uint64_t) * V, g->stream));
         GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
         GIR_CUDA(g, cudaMemcpyAsync(sbeg, set_beg_h + g0, sizeof(int64_t) * (nl + 1), cudaMemcpyHostToDevice, g->stream));
         const int64_t n_entries = set_beg_h[g0 + nl] - set_beg_h[g0];
@@ -359,11 +646,15 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
         double mu = (double)E - mf;                  // out-edges not yet explored (per lane)
         st.edges += (int64_t)hc[C_MEDGES];
         st.reached += (int64_t)hc[C_PAIRS];
-        bool bottom_up = false, next_dirty = false;
+        bool bottom_up = false, next_dirty = false, handed_back = false;
+        int pending = -1;  // a direction already decided (by the persistent launch) for this level
         int32_t L = 0;
         while (nq > 0) {
             // direction (the reference's switch, gir_query.cpp:159-169, or the schedule network)
-            if (learned) {  // decided on the device with the counters just read
+            if (pending >= 0) {
+                bottom_up = pending != 0;
+                pending = -1;
+            } else if (learned) {  // decided on the device with the counters just read
                 bottom_up = hc[C_DIR] != 0;
                 sched_trace(g, reinterpret_cast<const float*>(&hc[C_FEAT]), bottom_up ? 1 : 0);
             } else if (V >= 4096) {
@@ -373,6 +664,85 @@ int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t
                 else if (bottom_up && nf * beta < (double)V) bottom_up = false;
                 sched_trace(g, feat, bottom_up ? 1 : 0);
             }
+            // a small top-down frontier: levels run on the device until the launch hands back
+            if (!bottom_up && persist_grid > 0 && !handed_back && mf * nl <= (double)(1 << 24)) {
+                if (next_dirty) {
+                    GIR_CUDA(g, cudaMemsetAsync(next, 0, sizeof(uint64_t) * V, g->stream));
+                    next_dirty = false;
+                }
+                GIR_CUDA(g, cudaMemsetAsync(pctl, 0, sizeof(unsigned long long) * kCtlWords, g->stream));
+                PersistArgs pa;
+                pa.fw = view(g->fw);
+                pa.seen = seen;
+                pa.next = next;
+                pa.front[0] = front;
+                pa.front[1] = front2;
+                pa.q[0] = qa;
+                pa.q[1] = qb;
+                pa.q[2] = q3;
+                pa.level = level;
+                pa.V = V;
+                pa.nq0 = nq;
+                pa.E = (double)E;
+                pa.mf0 = mf;
+                pa.nf0 = nf;
+                pa.mu0 = mu;
+                pa.alpha = alpha;
+                pa.beta = beta;
+                pa.lanes = nl;
+                pa.L0 = L;
+                pa.max_levels = 1 << 30;
+                pa.net = learned ? net : nullptr;
+                pa.ctl = pctl;
+                pa.bar = reinterpret_cast<unsigned int*>(pctl + kCtlBarrier);
+                pa.trace = ptrace;
+                void* kargs[] = {&pa};
+                GIR_TRY(timer.run([&]() -> int {
+                    GIR_CUDA(g, cudaLaunchCooperativeKernel((const void*)k_bfs_persistent, persist_grid, kPersistThreads,
+                                                            kargs, 0, g->stream));
+                    return GIR_OK;
+                }));
+                st.launches++;
+                unsigned long long* pc = hc + 16;
+                GIR_CUDA(g, cudaMemcpyAsync(pc, pctl, sizeof(unsigned long long) * 16, cudaMemcpyDeviceToHost, g->stream));
+                GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+                if (pc[P_ERR]) return fail(g, GIR_ERR_TIMEOUT, "bfs: the persistent level loop ran out its barrier bound");
+                const int64_t lv = (int64_t)pc[P_LEVELS];
+                const int64_t n_tr = std::min<int64_t>(lv + (pc[P_REASON] == R_DONE ? 0 : 1), kPersistTrace);
+                if (n_tr > 0) {  // the schedule decisions taken inside the launch
+                    trace_rows.resize((size_t)n_tr * (GIR_SCHED_IN + 1));
+                    GIR_CUDA(g, cudaMemcpyAsync(trace_rows.data(), ptrace, sizeof(float) * trace_rows.size(),
+                                                cudaMemcpyDeviceToHost, g->stream));
+                    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+                    for (int64_t r = 0; r < n_tr; ++r) {
+                        const float* row = trace_rows.data() + r * (GIR_SCHED_IN + 1);
+                        sched_trace(g, row, (int32_t)row[GIR_SCHED_IN]);
+                    }
+                }
+                L += (int32_t)lv;
+                st.iterations += lv;
+                st.persistent_levels += lv;
+                st.edges += (int64_t)pc[P_EDGES];
+                st.reached += (int64_t)pc[P_REACHED];
+                nq = (int64_t)pc[P_NQ];
+                double d3[3];
+                std::memcpy(&d3[0], &pc[P_MF], sizeof(double));
+                std::memcpy(&d3[1], &pc[P_NF], sizeof(double));
+                std::memcpy(&d3[2], &pc[P_MU], sizeof(double));
+                mf = d3[0];
+                nf = d3[1];
+                mu = d3[2];
+                if (pc[P_FI]) std::swap(front, front2);
+                int32_t* qs[3] = {qa, qb, q3};
+                const int qi = (int)pc[P_QI];
+                qa = qs[qi];
+                qb = qs[(qi + 1) % 3];
+                q3 = qs[(qi + 2) % 3];
+                pending = (int)pc[P_DIR];
+                handed_back = pc[P_REASON] != R_BOTTOM_UP;  // (a big frontier: one level on the host first)
+                continue;
+            }
+            handed_back = false;
             GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
             if (!bottom_up) {
                 if (next_dirty) {

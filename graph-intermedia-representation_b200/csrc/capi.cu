@@ -937,6 +937,7 @@ int gir_dev_query_stats(gir_dev_t* g, gir_dev_query_stats_t* out) {
     out->total_ms = g->qstats.total_ms;
     out->main_ms = g->qstats.main_ms;
     out->main_launches = g->qstats.main_launches;
+    out->persistent_levels = g->qstats.persistent_levels;
     return GIR_OK;
 }
 

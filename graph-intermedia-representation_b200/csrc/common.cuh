@@ -64,6 +64,7 @@ struct QueryStats {
     int64_t edges = 0, reached = 0, iterations = 0, bottom_up = 0, launches = 0;
     double kernel_ms = 0, total_ms = 0, main_ms = 0;
     int64_t main_launches = 0;
+    int64_t persistent_levels = 0;
 };
 
 // Times the launches issued by `launch` with CUDA events when profiling is on, adding them to
@@ -347,6 +348,31 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t* q
     if (lane_id() == leader) base = atomicAdd(cnt, (unsigned long long)__popc(m));
     base = __shfl_sync(0xffffffffu, base, leader);
     if (pred) q[base + __popc(m & ((1u << lane_id()) - 1))] = value;
+}
+
+// Staged queue appends: a warp collects its entries in a shared-memory buffer of kStage slots
+// and reserves queue space with one atomicAdd per buffer-full, instead of one per ballot, so
+// thousands of warps appending to one queue do not serialize on its counter. Every lane of the
+// warp calls stage_append (warp-uniform), and stage_flush once at the end.
+constexpr int kStage = 128;
+__device__ __forceinline__ void stage_flush(int32_t* s_buf, int& s_n, int32_t* q, unsigned long long* cnt) {
+    if (s_n == 0) return;
+    unsigned long long base = 0;
+    if (lane_id() == 0) base = atomicAdd(cnt, (unsigned long long)s_n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (int i = lane_id(); i < s_n; i += 32) q[base + i] = s_buf[i];
+    __syncwarp();
+    s_n = 0;
+}
+__device__ __forceinline__ void stage_append(bool pred, int32_t value, int32_t* s_buf, int& s_n, int32_t* q,
+                                             unsigned long long* cnt) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    const int k = __popc(m);
+    if (s_n + k > kStage) stage_flush(s_buf, s_n, q, cnt);
+    if (pred) s_buf[s_n + __popc(m & ((1u << lane_id()) - 1))] = value;
+    __syncwarp();
+    s_n += k;
 }
 
 // Frontier expansion over one CSR: a warp takes 32 queue entries and walks their rows together.

@@ -19,69 +19,27 @@
 // kDirMargin; otherwise the fixed switch decides.
 // Parameter layout: W1[HID][IN], b1[HID], W2[OUT][HID], b2[OUT].
 #include "common.cuh"
+#include "sched_net.cuh"
 
 namespace gir {
 
 namespace {
 
-constexpr int IN = GIR_SCHED_IN, HID = GIR_SCHED_HID, OUT = GIR_SCHED_OUT;
-constexpr int NP = HID * IN + HID + OUT * HID + OUT;
+using namespace sched_net;
 constexpr int kBlock = 128;
 constexpr uint64_t kDeltaChoices[6] = {16, 32, 64, 256, 2048, 8192};
-constexpr float kDirMargin = 2.0f;
-
-struct Layout {
-    const float *W1, *b1, *W2, *b2;
-};
-__device__ __forceinline__ Layout layout(const float* p) {
-    return Layout{p, p + HID * IN, p + HID * IN + HID, p + HID * IN + HID + OUT * HID};
-}
-
-__device__ __forceinline__ void forward_one(const Layout& L, const float* x, float* h, float* o) {
-    for (int j = 0; j < HID; ++j) {
-        float z = L.b1[j];
-        for (int i = 0; i < IN; ++i) z += L.W1[j * IN + i] * x[i];
-        h[j] = tanhf(z);
-    }
-    for (int k = 0; k < OUT; ++k) {
-        float z = L.b2[k];
-        for (int j = 0; j < HID; ++j) z += L.W2[k * HID + j] * h[j];
-        o[k] = z;
-    }
-}
-
-// BFS level features (the host's sched_bfs_features and the device decision share it).
-__host__ __device__ inline void bfs_features(double V, double E, double nf, double mf, double mu, bool bottom_up,
-                                             int lanes, float* out) {
-    const double tiny = 1.0 / 4294967296.0;
-    out[0] = (float)(log2(nf / V + tiny) / 8.0);
-    out[1] = (float)((log2(mf + 1.0) - log2(mu + 1.0)) / 8.0);
-    out[2] = (float)(log2(mu / E + tiny) / 8.0);
-    out[3] = (float)(log2(mf / E + tiny) / 8.0);
-    out[4] = bottom_up ? 1.f : 0.f;
-    out[5] = (float)(log2(E / V + 1.0) / 8.0);
-    out[6] = (float)(lanes / 64.0);
-    out[7] = 0.f;  // task: BFS direction
-}
 
 // The next BFS level's direction, decided on the device from the level's counters (frontier
 // pairs and out-edges, summed over lanes), so the network costs no extra host round trip: the
 // decision and its features travel back with the counters the host reads anyway.
 __global__ void k_bfs_decide(const float* params, unsigned long long* cnt, int i_pairs, int i_medges, int i_dir,
                              int i_feat, int lanes, double V, double E, double mu_prev, int bottom_up, double alpha,
-                             double beta, float margin) {
+                             double beta) {
     if (threadIdx.x != 0) return;
     const double nf = (double)cnt[i_pairs] / lanes, mf = (double)cnt[i_medges] / lanes;
-    const double mu = mu_prev - mf;
-    float x[IN], h[HID], o[OUT];
-    bfs_features(V, E, nf, mf, mu, bottom_up != 0, lanes, x);
-    int fixed = bottom_up;
-    if (!bottom_up && mf * alpha > mu) fixed = 1;
-    else if (bottom_up && nf * beta < V) fixed = 0;
-    forward_one(layout(params), x, h, o);
-    const int net = o[1] > o[0] ? 1 : 0;
-    const float m = fabsf(o[1] - o[0]);
-    cnt[i_dir] = (unsigned long long)(m >= margin ? net : fixed);
+    float x[IN];
+    cnt[i_dir] = (unsigned long long)decide_direction(params, V, E, nf, mf, mu_prev - mf, bottom_up, lanes, alpha,
+                                                      beta, x);
     float* f = reinterpret_cast<float*>(&cnt[i_feat]);
     for (int i = 0; i < IN; ++i) f[i] = x[i];
 }
@@ -226,7 +184,7 @@ int sched_bfs_decide_async(gir_dev* g, unsigned long long* cnt, int i_pairs, int
     GIR_TRY(ensure_params(g, &p));
     k_bfs_decide<<<1, 32, 0, g->stream>>>(p, cnt, i_pairs, i_medges, i_dir, i_feat, lanes,
                                           (double)(g->V > 0 ? g->V : 1), (double)g->fw.E + 1.0, mu_prev,
-                                          bottom_up ? 1 : 0, alpha, beta, kDirMargin);
+                                          bottom_up ? 1 : 0, alpha, beta);
     GIR_LAUNCH(g, "k_bfs_decide");
     return GIR_OK;
 }

@@ -217,6 +217,8 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
     const int64_t n = (int64_t)*n_items;
     if (n == 0) return;
     const int64_t total = it.pref[n];
+    __shared__ int32_t s_near[kRelaxThreads / 32][kStage], s_far[kRelaxThreads / 32][kStage];
+    int n_near = 0, n_far = 0;
     const int ln = lane_id();
     const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -291,13 +293,15 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
                         }
                     }
                 }
-                warp_append(to_near, w[j], a.nextq, &a.cnt[S_NEAR]);
-                warp_append(to_far, w[j], a.farq, &a.cnt[S_FAR]);
+                stage_append(to_near, w[j], s_near[threadIdx.x >> 5], n_near, a.nextq, &a.cnt[S_NEAR]);
+                stage_append(to_far, w[j], s_far[threadIdx.x >> 5], n_far, a.farq, &a.cnt[S_FAR]);
             }
         }
         p = wend;  // (the pairs of this window end exactly where item e0+32 begins)
         e0 += 32;
     }
+    stage_flush(s_near[threadIdx.x >> 5], n_near, a.nextq, &a.cnt[S_NEAR]);
+    stage_flush(s_far[threadIdx.x >> 5], n_far, a.farq, &a.cnt[S_FAR]);
 }
 
 // Splits the far entries at the bucket [lo, hi): lanes inside it become near work, later lanes
@@ -307,6 +311,8 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
                             const uint64_t* dist, int nl, uint64_t lo, uint64_t hi, unsigned long long* nearmask,
                             int32_t* nearq, int32_t* farq2, unsigned long long* cnt) {
     const int64_t n = (int64_t)*nfar;
+    __shared__ int32_t s_near[kBlock / 32][kStage], s_far[kBlock / 32][kStage];
+    int n_near = 0, n_far = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
         bool to_near = false, to_far = false;
@@ -330,14 +336,16 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
             to_far = keep != 0;
             if (nm) to_near = atomicOr(&nearmask[w], nm) == 0ull;
         }
-        warp_append(to_near, w, nearq, &cnt[S_NEAR]);
-        warp_append(to_far, w, farq2, &cnt[S_FAR2]);
+        stage_append(to_near, w, s_near[threadIdx.x >> 5], n_near, nearq, &cnt[S_NEAR]);
+        stage_append(to_far, w, s_far[threadIdx.x >> 5], n_far, farq2, &cnt[S_FAR2]);
         for (int o = 16; o; o >>= 1) {
             const unsigned long long t = __shfl_xor_sync(0xffffffffu, mn, o);
             mn = t < mn ? t : mn;
         }
         if (lane_id() == 0 && mn != kInf) atomicMin(&cnt[S_MIN], mn);
     }
+    stage_flush(s_near[threadIdx.x >> 5], n_near, nearq, &cnt[S_NEAR]);
+    stage_flush(s_far[threadIdx.x >> 5], n_far, farq2, &cnt[S_FAR2]);
 }
 
 // Reached (vertex, lane) pairs and their out-degrees (the traversed edges of the GTEPS figure).

@@ -51,7 +51,8 @@ class GirError(RuntimeError):
 class QueryStats(ctypes.Structure):
     _fields_ = [("edges", ctypes.c_int64), ("reached", ctypes.c_int64), ("iterations", ctypes.c_int64),
                 ("bottom_up", ctypes.c_int64), ("launches", ctypes.c_int64), ("kernel_ms", ctypes.c_double),
-                ("total_ms", ctypes.c_double), ("main_ms", ctypes.c_double), ("main_launches", ctypes.c_int64)]
+                ("total_ms", ctypes.c_double), ("main_ms", ctypes.c_double), ("main_launches", ctypes.c_int64),
+                ("persistent_levels", ctypes.c_int64)]
 
 
 _P = ctypes.c_void_p

@@ -214,6 +214,8 @@ typedef struct {
     double main_ms;         /* with GIR_PARAM_PROFILE: summed device time of the main kernel's
                                launches (BFS: expand + bottom-up kernels; SSSP: relax) */
     int64_t main_launches;  /* ... and their number */
+    int64_t persistent_levels;  /* BFS levels run inside the persistent top-down launch (small
+                                   frontiers of high-diameter graphs; no reference counterpart) */
 } gir_dev_query_stats_t;
 int gir_dev_query_stats(gir_dev_t* g, gir_dev_query_stats_t* out);
 

@@ -236,3 +236,33 @@ def test_autotune_keeps_results(pkg, s16):
     with pytest.raises(pkg.GirError):
         d.autotune(np.zeros(65, np.int32))
     d.close()
+
+
+def test_persistent_levels_on_a_lattice(pkg, orc):
+    """A high-diameter graph runs most BFS levels inside the persistent top-down launch; levels
+    equal the oracle's, with the fixed switch and with the learned schedule, for single sources
+    and multi-source sets, and the schedule trace still holds a decision per level."""
+    lat = pkg.graphs.lattice(side=300, seed=12)
+    fb, fa = orc.normalize(lat.V, lat.fw_beg, lat.fw_adj)
+    d = pkg.DeviceGraph.from_graph(lat)
+    src = pkg.graphs.sources_with_edges(lat, 64, 5)
+    exp = np.stack([orc.bfs(lat.V, fb, fa, [s]) for s in src[:8]])
+    for mode in ("fixed", "top-down", "learned"):
+        if mode == "top-down":  # a tiny alpha never switches: every level can run persistent
+            d.set_param(pkg.native.PARAM_ALPHA, 1e-6)
+        if mode == "learned":
+            d.set_param(pkg.native.PARAM_ALPHA, 15)
+            d.use_learned_schedule()
+        lv = d.bfs(src)
+        st = d.query_stats()
+        assert st["persistent_levels"] > 0, st
+        if mode == "top-down":
+            assert st["persistent_levels"] > 0.9 * st["iterations"] and st["bottom_up"] <= 2, st
+        np.testing.assert_array_equal(lv[:8], exp)
+        x, y = d.sched_trace()
+        assert len(y) >= st["iterations"] and x.shape[1] == pkg.native.SCHED_IN
+        sets = [src[:3], src[3:4], src[4:40]]
+        ls = d.bfs_sets(sets)
+        for i, s in enumerate(sets):
+            np.testing.assert_array_equal(ls[i], orc.bfs(lat.V, fb, fa, list(s)))
+    d.close()

@@ -55,6 +55,8 @@ __global__ void k_h_deg(int64_t V, const int32_t* scc, const uint8_t* nontrivial
 // Forest roots: every SCC's smallest vertex; only those of non-singleton SCCs start the BFS.
 __global__ void k_roots(int64_t V, const int32_t* scc, const uint8_t* nontrivial, int32_t* parent, int32_t* depth,
                         int32_t* order, unsigned long long* cnt) {
+    __shared__ int32_t s_st[kBlock / 32][kStage];
+    int n_st = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t v = base + threadIdx.x;
         bool root = false;
@@ -64,8 +66,9 @@ __global__ void k_roots(int64_t V, const int32_t* scc, const uint8_t* nontrivial
             parent[v] = r ? (int32_t)v : -1;
             depth[v] = r ? 0 : -1;
         }
-        warp_append(root, (int32_t)v, order, &cnt[C_Q]);
+        stage_append(root, (int32_t)v, s_st[threadIdx.x >> 5], n_st, order, &cnt[C_Q]);
     }
+    stage_flush(s_st[threadIdx.x >> 5], n_st, order, &cnt[C_Q]);
 }
 
 // One BFS level of the spanning forest: the level's vertices are order[lo, lo + n); new ones are
@@ -81,6 +84,8 @@ constexpr int kForestChunk = 32 * 16;
 __global__ void __launch_bounds__(kBlock) k_forest_balanced(const int32_t* q, int64_t nq, const int64_t* pref, HView h,
                                                             int32_t* parent, int32_t* depth, int32_t L, int32_t* out,
                                                             unsigned long long* cnt) {
+    __shared__ int32_t s_st[kBlock / 32][kStage];
+    int n_st = 0;
     const int64_t total = pref[nq];
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -107,9 +112,10 @@ __global__ void __launch_bounds__(kBlock) k_forest_balanced(const int32_t* q, in
                     push = true;
                 }
             }
-            warp_append(push, w, out, &cnt[C_Q]);
+            stage_append(push, w, s_st[threadIdx.x >> 5], n_st, out, &cnt[C_Q]);
         }
     }
+    stage_flush(s_st[threadIdx.x >> 5], n_st, out, &cnt[C_Q]);
 }
 
 __global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) { GRID_STRIDE(i, n) p[i] = v; }

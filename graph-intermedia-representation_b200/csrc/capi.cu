@@ -271,15 +271,20 @@ int create_impl(const int32_t* fw_beg, const int32_t* fw_adj, const int32_t* bw_
                                               std::to_string(e_fw) + " vs " + std::to_string(e_bw) + " edges)");
     g->has_weights = w != nullptr;
     GIR_TRY(store_build_sym(g));
-    // Prime the pool with one block the size of the layer builds' largest working set (sort keys
-    // and their double buffers over the symmetrized capacity), so the first build and the first
-    // large batch do not map new memory piece by piece. At most a quarter of the free memory.
+    // Prime the pool with one block the size of the working set, so the first build, batch and
+    // query do not map new memory piece by piece. At most a quarter of the free memory.
     {
         size_t free_b = 0, total_b = 0;
         GIR_CUDA(g, cudaMemGetInfo(&free_b, &total_b));
         uint64_t reserved = 0;
         GIR_CUDA(g, cudaMemPoolGetAttribute(g->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
-        size_t want = (size_t)(24 * g->sym.cap + 64 * V);
+        // the working set: build sort keys (24 bytes per symmetric slot) and the query buffers
+        // (64 lanes of SSSP distances, BFS and SSSP output staging, masks and queues: ~3 KB per
+        // vertex, the high-water mark measured on a 4.8M-vertex graph); calls return their large
+        // buffers to the pool after use when it would take a third of free memory
+        const double need = 24.0 * (double)g->sym.cap + 3072.0 * (double)V;
+        g->scratch_tight = need > (double)free_b / 3.0;
+        size_t want = (size_t)need;
         want = want < free_b / 4 ? want : free_b / 4;
         if (want > reserved) {
             void* p = nullptr;

@@ -113,6 +113,7 @@ struct gir_dev {
     // on the handle's stream and the pool keeps its memory, so no call waits for the device to
     // go idle the way cudaMalloc / cudaFree do.
     cudaMemPool_t pool = nullptr;
+    bool scratch_tight = false;  // the graph's working set is large against free memory (see create)
 
     // Scratch, grown on demand and kept across calls.
     gir::DevBuf scratch[16];
@@ -184,9 +185,10 @@ int ensure_n(gir_dev* g, DevBuf& b, size_t n, T** out) {
     return GIR_OK;
 }
 void release(gir_dev* g, DevBuf& b);
-// Returns every working buffer of at least `min_bytes` to the handle's pool (top-level calls do
-// this on return: the pool hands the memory to the next phase that needs it, so the phases share
-// one working set instead of each keeping its own high-water mark).
+// When device memory is tight for the graph (scratch_tight, decided at create), returns every working buffer of at least
+// `min_bytes` to the handle's pool (top-level calls do this on return: the pool hands the memory
+// to the next phase that needs it, so on large graphs the phases share one working set instead of
+// each keeping its own high-water mark). Otherwise the buffers are kept for the next call.
 void release_scratch(gir_dev* g, size_t min_bytes);
 constexpr size_t kKeepScratchBelow = 64u << 20;
 
@@ -375,6 +377,29 @@ __device__ __forceinline__ void stage_append(bool pred, int32_t value, int32_t* 
     s_n += k;
 }
 
+// Slots for the CTA's flagged threads with one atomicAdd for the whole CTA (block-uniform call;
+// s_w: shared int[blockDim / 32], s_base: one shared word). Returns this thread's slot.
+__device__ __forceinline__ unsigned long long block_slot(bool pred, unsigned long long* cnt, int* s_w,
+                                                         unsigned long long* s_base) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    const int wib = threadIdx.x >> 5;
+    if (lane_id() == 0) s_w[wib] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            const int c = s_w[k];
+            s_w[k] = tot;
+            tot += c;
+        }
+        *s_base = tot ? atomicAdd(cnt, (unsigned long long)tot) : 0ull;
+    }
+    __syncthreads();
+    const unsigned long long slot = *s_base + (unsigned long long)s_w[wib] + __popc(m & ((1u << lane_id()) - 1));
+    __syncthreads();  // (s_w and s_base are rewritten by the next call)
+    return slot;
+}
+
 // Frontier expansion over one CSR: a warp takes 32 queue entries and walks their rows together.
 // f(u, w) is called for every entry w of row u; it returns true when w joins the next queue.
 template <class F>
@@ -383,6 +408,8 @@ __device__ __forceinline__ void warp_expand(const int32_t* q, int64_t n, const C
     constexpr int kW = 32;  // supports blocks of up to 1024 threads
     __shared__ int64_t s_excl[kW][33];
     __shared__ int32_t s_u[kW][32];
+    __shared__ int32_t s_st[kW][kStage];
+    int n_st = 0;
     const int lane = lane_id(), wib = threadIdx.x >> 5;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -414,10 +441,11 @@ __device__ __forceinline__ void warp_expand(const int32_t* q, int64_t n, const C
                 w = c.adj[c.beg[uu] + (p - s_excl[wib][lo])];
                 push = f(uu, w);
             }
-            warp_append(push, w, nq, ncnt);
+            stage_append(push, w, s_st[wib], n_st, nq, ncnt);
         }
         __syncwarp();
     }
+    stage_flush(s_st[wib], n_st, nq, ncnt);
 }
 
 #endif

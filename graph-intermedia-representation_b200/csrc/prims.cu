@@ -64,6 +64,7 @@ int ensure(gir_dev* g, DevBuf& b, size_t bytes) {
 }
 
 void release_scratch(gir_dev* g, size_t min_bytes) {
+    if (!g->scratch_tight) return;  // memory is not tight: keep the buffers for the next call
     auto drop = [&](DevBuf& b) {
         if (b.p && b.bytes >= min_bytes) release(g, b);
     };

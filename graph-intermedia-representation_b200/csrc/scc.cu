@@ -36,6 +36,8 @@ enum { C_Q = 0, C_ACT = 1, C_ROOTS = 2, C_PIV = 3, C_N = 8 };
 // Active in/out degree counts (self-loops excluded) and the first trim frontier.
 __global__ void k_trim_init(int64_t V, CSRView fw, CSRView bw, int32_t* label, int32_t* indeg, int32_t* outdeg,
                             int32_t* q, unsigned long long* cnt) {
+    __shared__ int32_t s_st[kBlock / 32][kStage];
+    int n_st = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t v = base + threadIdx.x;
         bool trim = false;
@@ -50,8 +52,9 @@ __global__ void k_trim_init(int64_t V, CSRView fw, CSRView bw, int32_t* label, i
             trim = (o == 0 || in == 0);
             label[v] = trim ? (int32_t)v : -1;
         }
-        warp_append(trim, (int32_t)v, q, &cnt[C_Q]);
+        stage_append(trim, (int32_t)v, s_st[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
     }
+    stage_flush(s_st[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
 }
 
 // One trim round over the removed vertices of the last round: lower the counts of their
@@ -115,6 +118,8 @@ template <bool Backward>
 __global__ void __launch_bounds__(kBlock) k_reach_balanced(const int32_t* q, int64_t nq, const int64_t* pref, CSRView c,
                                                            int32_t* label, int32_t* mark, int32_t epoch, int32_t pivot,
                                                            int32_t* out, unsigned long long* cnt) {
+    __shared__ int32_t s_st[kBlock / 32][kStage];
+    int n_st = 0;
     const int64_t total = pref[nq];
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -142,20 +147,24 @@ __global__ void __launch_bounds__(kBlock) k_reach_balanced(const int32_t* q, int
                     if (mark[w] == epoch && label[w] == -1) push = atomicCAS(&label[w], -1, pivot) == -1;
                 }
             }
-            warp_append(push, w, out, &cnt[C_Q]);
+            stage_append(push, w, s_st[threadIdx.x >> 5], n_st, out, &cnt[C_Q]);
         }
     }
+    stage_flush(s_st[threadIdx.x >> 5], n_st, out, &cnt[C_Q]);
 }
 
 // Colour propagation: colour(w) = max(colour(w), colour(u)) along forward edges between
 // unassigned vertices. `inq` de-duplicates the next queue per round.
 __global__ void k_color_init(int64_t V, const int32_t* label, int32_t* color, int32_t* q, unsigned long long* cnt) {
+    __shared__ int32_t s_st[kBlock / 32][kStage];
+    int n_st = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t v = base + threadIdx.x;
         const bool on = v < V && label[v] == -1;
         if (v < V) color[v] = (int32_t)v;
-        warp_append(on, (int32_t)v, q, &cnt[C_Q]);
+        stage_append(on, (int32_t)v, s_st[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
     }
+    stage_flush(s_st[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
 }
 
 __global__ void __launch_bounds__(kBlock) k_color_prop(const int32_t* q, const unsigned long long* qlen, CSRView fw,
@@ -171,6 +180,8 @@ __global__ void __launch_bounds__(kBlock) k_color_prop(const int32_t* q, const u
 }
 
 __global__ void k_color_roots(int64_t V, int32_t* label, const int32_t* color, int32_t* q, unsigned long long* cnt) {
+    __shared__ int32_t s_st[kBlock / 32][kStage];
+    int n_st = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < V; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t v = base + threadIdx.x;
         bool root = false;
@@ -178,8 +189,9 @@ __global__ void k_color_roots(int64_t V, int32_t* label, const int32_t* color, i
             label[v] = (int32_t)v;
             root = true;
         }
-        warp_append(root, (int32_t)v, q, &cnt[C_Q]);
+        stage_append(root, (int32_t)v, s_st[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
     }
+    stage_flush(s_st[threadIdx.x >> 5], n_st, q, &cnt[C_Q]);
 }
 
 // Backward search inside each colour class from its root.
@@ -397,7 +409,7 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
         }));
     }
 
-    if (g->trace_on) std::fprintf(stderr, "[gir] scc: colour rounds %d\n", (int)round);
+    if (g->trace_marks) std::fprintf(stderr, "[gir] scc: colour rounds %d\n", (int)round);
     trace_mark(g, "scc: colour");
     // 4. canonical labels
     int32_t* mn = color;

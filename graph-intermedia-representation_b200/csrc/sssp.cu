@@ -149,6 +149,8 @@ __global__ void k_light_split(int64_t V, const int64_t* wb, const int32_t* wdeg,
 // item count goes to cnt[S_ITEMS]. Item slots past the count keep the zero work they were
 // cleared to, so a scan over all n + 1 slots needs no count from the host.
 __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, const int32_t* nlight, Items it) {
+    __shared__ int s_w[kBlock / 32];
+    __shared__ unsigned long long s_base;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
         int32_t u = 0;
@@ -170,20 +172,15 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
             eb = heavy ? b + nlu : b;
             work = (int64_t)(heavy ? a.wdeg[u] - nlu : nlu) * __popcll(m);
         }
-        warp_append(settles, u, a.setq, &a.cnt[S_SET]);
+        const unsigned long long ss = block_slot(settles, &a.cnt[S_SET], s_w, &s_base);
+        if (settles) a.setq[ss] = u;
         const bool has = work > 0;
-        const unsigned bal = __ballot_sync(0xffffffffu, has);
-        if (bal) {
-            const int leader = __ffs(bal) - 1;
-            unsigned long long slot = 0;
-            if (lane_id() == leader) slot = atomicAdd(&a.cnt[S_ITEMS], (unsigned long long)__popc(bal));
-            slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(bal & ((1u << lane_id()) - 1));
-            if (has) {
-                it.u[slot] = u;
-                it.eb[slot] = eb;
-                it.m[slot] = m;
-                it.pref[slot] = work;
-            }
+        const unsigned long long slot = block_slot(has, &a.cnt[S_ITEMS], s_w, &s_base);
+        if (has) {
+            it.u[slot] = u;
+            it.eb[slot] = eb;
+            it.m[slot] = m;
+            it.pref[slot] = work;
         }
     }
 }
@@ -536,7 +533,7 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
             k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, nlight, items);
             GIR_LAUNCH(g, "k_relax_prep");
             GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));
-            if (g->trace_on) {
+            if (g->trace_marks) {
                 int64_t tot = 0;
                 GIR_CUDA(g, cudaMemcpyAsync(&tot, items.pref + n, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
                 GIR_CUDA(g, cudaStreamSynchronize(g->stream));
@@ -601,7 +598,7 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
             }
             if (finished) break;
         }
-        if (g->trace_on)
+        if (g->trace_marks)
             std::fprintf(stderr, "[gir] sssp group of %d lanes, delta %llu: %lld passes, %lld (edge, lane) pairs\n", nl,
                          (unsigned long long)D, (long long)trace_passes, (long long)trace_pairs);
         k_sssp_reached<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(dist, V, nl, g->fw.deg, cnt);

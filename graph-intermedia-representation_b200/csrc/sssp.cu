@@ -80,7 +80,8 @@ __global__ void k_deg_i64(int64_t V, const int32_t* deg, int64_t* out) {
 }
 
 // Lane s of the group starts at every vertex of set s (set_beg: device copy, absolute offsets).
-__global__ void k_sssp_init(const int64_t* set_beg, int nl, const int32_t* srcs, int64_t V, uint64_t* dist,
+template <class D>
+__global__ void k_sssp_init(const int64_t* set_beg, int nl, const int32_t* srcs, int64_t V, D* dist,
                             unsigned long long* nearmask, int32_t* nearq, unsigned long long* cnt) {
     const int64_t lo = set_beg[0], hi = set_beg[nl];
     GRID_STRIDE(i, hi - lo) {
@@ -93,6 +94,23 @@ __global__ void k_sssp_init(const int64_t* set_beg, int nl, const int32_t* srcs,
         if (atomicOr(&nearmask[v], 1ull << s) == 0ull) nearq[atomicAdd(&cnt[S_NEAR], 1ull)] = v;
     }
 }
+
+// Distances inside a lane group are uint32 when every finite distance fits ((V - 1) * max weight
+// < 2^32 - 1): half the bytes, eight lanes per 32-byte sector, 32-bit atomics. Output is uint64.
+template <class D>
+struct DistT;
+template <>
+struct DistT<uint64_t> {
+    static constexpr uint64_t inf = ~0ull;
+    __device__ static uint64_t atomic_min(uint64_t* p, uint64_t v) {
+        return atomicMin((unsigned long long*)p, (unsigned long long)v);
+    }
+};
+template <>
+struct DistT<uint32_t> {
+    static constexpr uint32_t inf = ~0u;
+    __device__ static uint32_t atomic_min(uint32_t* p, uint32_t v) { return atomicMin((unsigned int*)p, v); }
+};
 
 // Index of the k-th set bit of a 64-bit mask (k < popcount).
 __device__ __forceinline__ int nth_bit(uint64_t m, int k) {
@@ -109,7 +127,7 @@ struct Relax {
     const uint32_t* ww;
     uint64_t delta, kend;    // bucket width; end of the current bucket
     int nl;                  // lanes (row stride of dist)
-    uint64_t* dist;
+    void* dist;              // lane distances (uint32 or uint64, see DistT)
     unsigned long long* curmask;   // lanes of each queued vertex to process (read and cleared)
     unsigned long long* nextmask;  // lanes re-entering the bucket
     int32_t* nextq;
@@ -210,7 +228,9 @@ __device__ __forceinline__ int64_t warp_search(const int64_t* pref, int64_t lo, 
 // window through shuffles, so no shared memory and no block barrier is involved and warps
 // proceed independently. Pairs are enumerated edge-major within an item: with many lanes
 // active, consecutive threads update consecutive lanes of one distance row.
+template <class D>
 __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long long* n_items, Items it, Relax a) {
+    D* const dist = static_cast<D*>(a.dist);
     const int64_t n = (int64_t)*n_items;
     if (n == 0) return;
     const int64_t total = it.pref[n];
@@ -263,7 +283,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
                     const int32_t q2 = (int32_t)(q - px);
                     k[j] = ebx + q2 / pc;
                     sl[j] = nth_bit(mx, q2 % pc);
-                    du[j] = a.dist[(int64_t)ux * a.nl + sl[j]];
+                    du[j] = dist[(int64_t)ux * a.nl + sl[j]];
                 }
             }
             uint32_t wt[kPairs];
@@ -274,15 +294,14 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
             uint64_t cur[kPairs];
 #pragma unroll
             for (int j = 0; j < kPairs; ++j)
-                cur[j] = on[j] ? *(volatile uint64_t*)&a.dist[(int64_t)w[j] * a.nl + sl[j]] : 0ull;
+                cur[j] = on[j] ? *(volatile D*)&dist[(int64_t)w[j] * a.nl + sl[j]] : (D)0;
 #pragma unroll
             for (int j = 0; j < kPairs; ++j) {
                 bool to_near = false, to_far = false;
                 if (on[j]) {
                     const uint64_t nd = du[j] + (uint64_t)wt[j];
                     if (nd < cur[j]) {  // plain pre-check: most relaxations lose
-                        const unsigned long long old = atomicMin(
-                            (unsigned long long*)&a.dist[(int64_t)w[j] * a.nl + sl[j]], (unsigned long long)nd);
+                        const uint64_t old = DistT<D>::atomic_min(&dist[(int64_t)w[j] * a.nl + sl[j]], (D)nd);
                         if (nd < old) {
                             const unsigned long long bit = 1ull << sl[j];
                             if (nd < a.kend) to_near = atomicOr(&a.nextmask[w[j]], bit) == 0ull;
@@ -304,8 +323,9 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
 // Splits the far entries at the bucket [lo, hi): lanes inside it become near work, later lanes
 // stay far (queued in farq2) and their smallest distance goes to cnt[S_MIN] (the bucket to jump
 // to when this one turns out empty); settled lanes are dropped.
+template <class D>
 __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar, unsigned long long* farmask,
-                            const uint64_t* dist, int nl, uint64_t lo, uint64_t hi, unsigned long long* nearmask,
+                            const D* dist, int nl, uint64_t lo, uint64_t hi, unsigned long long* nearmask,
                             int32_t* nearq, int32_t* farq2, unsigned long long* cnt) {
     const int64_t n = (int64_t)*nfar;
     __shared__ int32_t s_near[kBlock / 32][kStage], s_far[kBlock / 32][kStage];
@@ -346,12 +366,13 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
 }
 
 // Reached (vertex, lane) pairs and their out-degrees (the traversed edges of the GTEPS figure).
-__global__ void k_sssp_reached(const uint64_t* dist, int64_t V, int nl, const int32_t* outdeg,
+template <class D>
+__global__ void k_sssp_reached(const D* dist, int64_t V, int nl, const int32_t* outdeg,
                                unsigned long long* cnt) {
     unsigned long long r = 0, e = 0;
     GRID_STRIDE(v, V) {
         unsigned c = 0;
-        for (int s = 0; s < nl; ++s) c += dist[v * nl + s] != kInf;
+        for (int s = 0; s < nl; ++s) c += dist[v * nl + s] != DistT<D>::inf;
         r += c;
         e += (unsigned long long)c * (unsigned long long)outdeg[v];
     }
@@ -366,7 +387,8 @@ __global__ void k_sssp_reached(const uint64_t* dist, int64_t V, int nl, const in
 }
 
 // dist[v * nl + s] -> out[s * V + v], through 32 x 32 shared-memory tiles.
-__global__ void k_transpose(const uint64_t* dist, int64_t V, int nl, uint64_t* out) {
+template <class D>
+__global__ void k_transpose(const D* dist, int64_t V, int nl, uint64_t* out) {
     __shared__ uint64_t tile[32][33];
     const int64_t v0 = (int64_t)blockIdx.x * 32;
     const int s0 = blockIdx.y * 32;
@@ -374,7 +396,10 @@ __global__ void k_transpose(const uint64_t* dist, int64_t V, int nl, uint64_t* o
     for (int r = ty; r < 32; r += 8) {
         const int64_t v = v0 + r;
         const int s = s0 + tx;
-        if (v < V && s < nl) tile[r][tx] = dist[v * nl + s];
+        if (v < V && s < nl) {
+            const D d = dist[v * nl + s];
+            tile[r][tx] = d == DistT<D>::inf ? kInf : (uint64_t)d;
+        }
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
@@ -474,9 +499,14 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
     const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
     MainTimer timer{g, g->params[GIR_PARAM_PROFILE] != 0.0};
     // the relaxation kernel gives every warp one contiguous run of pairs: one CTA per resident slot
-    int per_sm = 0;
-    GIR_CUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_relax, kRelaxThreads, 0));
-    const int run_grid = g->num_sms * (per_sm > 0 ? per_sm : 1);
+    int per_sm = 0, per_sm32 = 0;
+    GIR_CUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_relax<uint64_t>, kRelaxThreads, 0));
+    GIR_CUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_relax<uint32_t>, kRelaxThreads, 0));
+    const int run_grid64 = g->num_sms * (per_sm > 0 ? per_sm : 1);
+    const int run_grid32 = g->num_sms * (per_sm32 > 0 ? per_sm32 : 1);
+    // uint32 lane distances when every finite distance fits
+    const double wmax = g->wstat[hash ? 0 : 1][1] > 0 ? g->wstat[hash ? 0 : 1][1] : 4294967295.0;
+    const bool fits32 = (double)V * wmax < 4294967295.0;
     int32_t* nlight = nullptr;
     GIR_TRY(ensure_n(g, g->scratch[9], V + 1, &nlight));
     Items items;
@@ -493,8 +523,10 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         GIR_CUDA(g, cudaMemsetAsync(nextmask, 0, sizeof(unsigned long long) * V, g->stream));
         GIR_CUDA(g, cudaMemsetAsync(farmask, 0, sizeof(unsigned long long) * V, g->stream));
         GIR_CUDA(g, cudaMemsetAsync(setmask, 0, sizeof(unsigned long long) * V, g->stream));
-        uint64_t* dist = nl > 1 ? idist : dist_d + g0 * V;
-        if (nl > 1) GIR_CUDA(g, cudaMemsetAsync(dist, 0xff, sizeof(uint64_t) * V * nl, g->stream));
+        const bool narrow = nl > 1 && fits32;  // (one lane writes the uint64 output in place)
+        void* dist = nl > 1 ? (void*)idist : (void*)(dist_d + g0 * V);
+        if (nl > 1)
+            GIR_CUDA(g, cudaMemsetAsync(dist, 0xff, (narrow ? sizeof(uint32_t) : sizeof(uint64_t)) * V * nl, g->stream));
         uint64_t D = delta;
         float feat[GIR_SCHED_IN];
         sched_sssp_features(g, weight_mode, nl, feat);
@@ -513,8 +545,12 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, g->stream));
         const int64_t n_entries = set_beg_h[g0 + nl] - set_beg_h[g0];
         if (n_entries > 0) {
-            k_sssp_init<<<grid_for(g, n_entries, kBlock), kBlock, 0, g->stream>>>(sbeg, nl, srcs_d, V, dist, curmask,
-                                                                                 nearq, cnt);
+            if (narrow)
+                k_sssp_init<uint32_t><<<grid_for(g, n_entries, kBlock), kBlock, 0, g->stream>>>(
+                    sbeg, nl, srcs_d, V, static_cast<uint32_t*>(dist), curmask, nearq, cnt);
+            else
+                k_sssp_init<uint64_t><<<grid_for(g, n_entries, kBlock), kBlock, 0, g->stream>>>(
+                    sbeg, nl, srcs_d, V, static_cast<uint64_t*>(dist), curmask, nearq, cnt);
             GIR_LAUNCH(g, "k_sssp_init");
         }
         GIR_TRY(read());
@@ -541,7 +577,10 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
                 ++trace_passes;
             }
             GIR_TRY(timer.run([&]() -> int {
-                k_relax<<<run_grid, kRelaxThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
+                if (narrow)
+                    k_relax<uint32_t><<<run_grid32, kRelaxThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
+                else
+                    k_relax<uint64_t><<<run_grid64, kRelaxThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
                 GIR_LAUNCH(g, "k_relax");
                 return GIR_OK;
             }));
@@ -579,8 +618,14 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
                 k = lo / D;
                 GIR_CUDA(g, cudaMemsetAsync(cnt + S_MIN, 0xff, sizeof(unsigned long long), g->stream));
                 GIR_CUDA(g, cudaMemsetAsync(cnt + S_FAR2, 0, sizeof(unsigned long long), g->stream));
-                k_far_split<<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(
-                    farq, cnt + S_FAR, farmask, dist, nl, k * D, (k + 1) * D, curmask, nearq, farq2, cnt);
+                if (narrow)
+                    k_far_split<uint32_t><<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(
+                        farq, cnt + S_FAR, farmask, static_cast<const uint32_t*>(dist), nl, k * D, (k + 1) * D, curmask,
+                        nearq, farq2, cnt);
+                else
+                    k_far_split<uint64_t><<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(
+                        farq, cnt + S_FAR, farmask, static_cast<const uint64_t*>(dist), nl, k * D, (k + 1) * D, curmask,
+                        nearq, farq2, cnt);
                 GIR_LAUNCH(g, "k_far_split");
                 st.launches++;
                 std::swap(farq, farq2);
@@ -601,11 +646,19 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         if (g->trace_marks)
             std::fprintf(stderr, "[gir] sssp group of %d lanes, delta %llu: %lld passes, %lld (edge, lane) pairs\n", nl,
                          (unsigned long long)D, (long long)trace_passes, (long long)trace_pairs);
-        k_sssp_reached<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(dist, V, nl, g->fw.deg, cnt);
+        if (narrow)
+            k_sssp_reached<uint32_t><<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(static_cast<const uint32_t*>(dist),
+                                                                                      V, nl, g->fw.deg, cnt);
+        else
+            k_sssp_reached<uint64_t><<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(static_cast<const uint64_t*>(dist),
+                                                                                      V, nl, g->fw.deg, cnt);
         GIR_LAUNCH(g, "k_sssp_reached");
         if (nl > 1) {
             dim3 grd((unsigned)((V + 31) / 32), (unsigned)((nl + 31) / 32));
-            k_transpose<<<grd, 256, 0, g->stream>>>(dist, V, nl, dist_d + g0 * V);
+            if (narrow)
+                k_transpose<uint32_t><<<grd, 256, 0, g->stream>>>(static_cast<const uint32_t*>(dist), V, nl, dist_d + g0 * V);
+            else
+                k_transpose<uint64_t><<<grd, 256, 0, g->stream>>>(static_cast<const uint64_t*>(dist), V, nl, dist_d + g0 * V);
             GIR_LAUNCH(g, "k_transpose");
         }
     }

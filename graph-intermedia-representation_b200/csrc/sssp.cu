@@ -149,16 +149,20 @@ struct Items {
 };
 
 // Number of light edges (weight < delta) of every weight-sorted row, once per query group.
+// Written with it, one 16-byte record per vertex for the queue bookkeeping of every pass: the
+// row start (two halves), its length and its light-edge count, so a queued vertex costs one
+// scattered load instead of three.
 __global__ void k_light_split(int64_t V, const int64_t* wb, const int32_t* wdeg, const uint32_t* ww, uint64_t delta,
-                              int32_t* nlight) {
+                              int4* rows) {
     GRID_STRIDE(v, V) {
-        const int64_t b = wb[v], e = b + wdeg[v];
-        int64_t lo = b, hi = e;
+        const int64_t b = wb[v];
+        const int32_t d = wdeg[v];
+        int64_t lo = b, hi = b + d;
         while (lo < hi) {
             const int64_t mid = (lo + hi) >> 1;
             if ((uint64_t)ww[mid] < delta) lo = mid + 1; else hi = mid;
         }
-        nlight[v] = (int32_t)(lo - b);
+        rows[v] = make_int4((int32_t)(uint32_t)b, (int32_t)(b >> 32), d, (int32_t)(lo - b));
     }
 }
 
@@ -166,7 +170,7 @@ __global__ void k_light_split(int64_t V, const int64_t* wb, const int32_t* wdeg,
 // item (vertex, first edge, lane mask, work = edges x lanes) for every vertex with work; the
 // item count goes to cnt[S_ITEMS]. Item slots past the count keep the zero work they were
 // cleared to, so a scan over all n + 1 slots needs no count from the host.
-__global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, const int32_t* nlight, Items it) {
+__global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, const int4* rows, Items it) {
     __shared__ int s_w[kBlock / 32];
     __shared__ unsigned long long s_base;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
@@ -185,10 +189,11 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
                 a.curmask[u] = 0ull;
                 settles = m && atomicOr(&a.setmask[u], m) == 0ull;
             }
-            const int64_t b = a.wb[u];
-            const int32_t nlu = nlight[u];
+            const int4 r = rows[u];
+            const int64_t b = (int64_t)(((uint64_t)(uint32_t)r.y << 32) | (uint32_t)r.x);
+            const int32_t nlu = r.w;
             eb = heavy ? b + nlu : b;
-            work = (int64_t)(heavy ? a.wdeg[u] - nlu : nlu) * __popcll(m);
+            work = (int64_t)(heavy ? r.z - nlu : nlu) * __popcll(m);
         }
         const unsigned long long ss = block_slot(settles, &a.cnt[S_SET], s_w, &s_base);
         if (settles) a.setq[ss] = u;
@@ -507,8 +512,8 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
     // uint32 lane distances when every finite distance fits
     const double wmax = g->wstat[hash ? 0 : 1][1] > 0 ? g->wstat[hash ? 0 : 1][1] : 4294967295.0;
     const bool fits32 = (double)V * wmax < 4294967295.0;
-    int32_t* nlight = nullptr;
-    GIR_TRY(ensure_n(g, g->scratch[9], V + 1, &nlight));
+    int4* rows = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[9], V + 1, &rows));
     Items items;
     GIR_TRY(ensure_n(g, g->qitems[0], V + 1, &items.u));
     GIR_TRY(ensure_n(g, g->qitems[1], V + 1, &items.eb));
@@ -561,12 +566,12 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         uint64_t k = 0;
         int64_t trace_pairs = 0, trace_passes = 0;
         // one relaxation pass over queue q (n entries): prep, scan of the work, balanced run
-        k_light_split<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, ws.beg, ws.deg, ws.w, D, nlight);
+        k_light_split<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, ws.beg, ws.deg, ws.w, D, rows);
         GIR_LAUNCH(g, "k_light_split");
         auto relax = [&](const int32_t* q, int64_t n, int heavy) -> int {
             GIR_CUDA(g, cudaMemsetAsync(cnt + S_ITEMS, 0, sizeof(unsigned long long), g->stream));
             GIR_CUDA(g, cudaMemsetAsync(items.pref, 0, sizeof(int64_t) * (n + 1), g->stream));
-            k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, nlight, items);
+            k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, rows, items);
             GIR_LAUNCH(g, "k_relax_prep");
             GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));
             if (g->trace_marks) {

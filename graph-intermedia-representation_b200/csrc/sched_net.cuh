@@ -12,7 +12,7 @@ constexpr int IN = GIR_SCHED_IN, HID = GIR_SCHED_HID, OUT = GIR_SCHED_OUT;
 constexpr int NP = HID * IN + HID + OUT * HID + OUT;
 // A BFS direction is taken from the network only when its two logits differ by at least this;
 // otherwise the fixed switch decides.
-constexpr float kDirMargin = 2.0f;
+constexpr float kDirMargin = 8.0f;
 
 struct Layout {
     const float *W1, *b1, *W2, *b2;

@@ -666,7 +666,7 @@ int gir_dev_destroy(gir_dev_t* g) {
     if (g->stream && g->pool) {
         store_free(g, g->fw); store_free(g, g->bw); store_free(g, g->sym);
         store_free(g, g->ws[0]); store_free(g, g->ws[1]);
-        for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
+        for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->dag_rows, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
                           &g->cub_tmp, &g->stage_in, &g->stage_out, &g->sched_w, &g->sched_io, &g->lane_dist})
             release(g, *b);
         for (auto& b : g->scratch) release(g, b);
@@ -850,6 +850,29 @@ int gir_dev_autotune(gir_dev_t* g, const int32_t* srcs, int64_t n_src, int reps,
     g->bins_valid = false;
     if (rc != GIR_OK) return rc;
     if (best_ms) *best_ms = best;
+    return GIR_OK;
+}
+
+int gir_dev_reachable(gir_dev_t* g, const int32_t* u, const int32_t* v, int64_t n, uint8_t* out) {
+    if (!g) return GIR_ERR_INVALID;
+    if (n < 0 || (n > 0 && (!u || !v || !out))) return fail(g, GIR_ERR_INVALID, "reachable: bad arguments");
+    if (!g->scc_built) return fail(g, GIR_ERR_STATE, "reachable needs buildSCC_DAG first");
+    if (n == 0) return GIR_OK;
+    DevBuf su, sv;
+    const void *du = nullptr, *dv = nullptr;
+    void* dout = nullptr;
+    int rc = GIR_OK;
+    if ((rc = stage_input(g, su, u, sizeof(int32_t) * n, &du)) || (rc = stage_input(g, sv, v, sizeof(int32_t) * n, &dv)) ||
+        (rc = out_target(g, out, (size_t)n, g->stage_out, &dout)) ||
+        (rc = reach_run(g, (const int32_t*)du, (const int32_t*)dv, n, (uint8_t*)dout)) ||
+        (rc = finish_out(g, out, dout, (size_t)n))) {
+        release(g, su);
+        release(g, sv);
+        return rc;
+    }
+    release(g, su);
+    release(g, sv);
+    release_scratch(g, kKeepScratchBelow);
     return GIR_OK;
 }
 

@@ -96,6 +96,8 @@ struct gir_dev {
     gir::DevBuf wcc, scc, scc_rank;  // int32[V]
     int64_t n_wcc = -1, n_scc = -1;
     gir::DevBuf dag;                 // uint64 keys (scc_u << 32 | scc_v), sorted, distinct
+    gir::DevBuf dag_rows;            // int64[V + 1]: row starts of dag by source label (reachability)
+    bool dag_rows_valid = false;
     int64_t n_dag = -1;
     gir::DevBuf blk_label, blk_head, bcnt;  // int32[V], int32[n_blocks], int32[V]
     int64_t n_blocks = -1;
@@ -252,6 +254,8 @@ int wcc_union_pairs(gir_dev* g, const uint64_t* keys, int64_t n);
 int scc_build(gir_dev* g);
 // Condensation DAG and ranks from the current SCC labels (the labels are kept).
 int scc_build_dag(gir_dev* g);
+// Reachability of every pair (u[i], v[i]) into out[i] (device arrays; the SCC layer is built).
+int reach_run(gir_dev* g, const int32_t* u_d, const int32_t* v_d, int64_t n, uint8_t* out_d);
 int bct_build(gir_dev* g);
 
 // ---- queries ----

@@ -466,6 +466,7 @@ int scc_build_dag(gir_dev* g) {
         GIR_TRY(select_flagged_u64(g, keys, flag, dag, n_cross, &n_dag));
     }
     g->n_dag = n_dag;
+    g->dag_rows_valid = false;
     trace_mark(g, "scc: dag edges");
 
     // topological ranks: longest-path levels over the condensation edges, rounds until stable

@@ -194,6 +194,16 @@ class DeviceGraph:
         return {"ctas_per_sm": self.get_param(P.PARAM_CTAS_PER_SM), "small_deg": self.get_param(P.PARAM_SMALL_DEG),
                 "large_deg": self.get_param(P.PARAM_LARGE_DEG), "bfs_ms": best.value}
 
+    def reachable(self, u, v, out=None):
+        """GIR::reachable for every pair (u[i], v[i]): a bool array (or fills `out`, uint8)."""
+        su, n = self._ids(u)
+        sv, n2 = self._ids(v)
+        if n != n2:
+            raise ValueError("reachable: u and v differ in length")
+        res = np.empty(n, np.uint8) if out is None else out
+        self._ck(dev_lib().gir_dev_reachable(self._h, ptr(su), ptr(sv), n, ptr(res)), "reachable")
+        return res.astype(bool) if out is None else res
+
     def batch_plan(self):
         """Per layer, what the last batch did: 'kept', 'patched' or 'rebuilt'."""
         out = np.zeros(3, np.int32)
@@ -421,6 +431,10 @@ class GIR:
 
     def sssp(self, source, delta=16):
         return self._d.sssp([source], delta=delta)[0]
+
+    def reachable(self, u, v):
+        """gir.h:128-130 (gir_query.cpp:789-825); batches go through DeviceGraph.reachable."""
+        return bool(self._d.reachable([u], [v])[0])
 
     @staticmethod
     def edgeWeight(u, v):

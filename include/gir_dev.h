@@ -170,6 +170,12 @@ int gir_dev_batch_plan(gir_dev_t* g, int32_t* plan3);
  * change. *best_ms (may be NULL) = the winner's device time per call. */
 int gir_dev_autotune(gir_dev_t* g, const int32_t* srcs, int64_t n_src, int reps, double* best_ms);
 
+/* GIR::reachable (gir_query.cpp:789-825) for a batch: out[i] = 1 iff v[i] is reachable from u[i]
+ * (1 for u == v; 0 for an id out of range). Needs the SCC layer (GIR_ERR_STATE otherwise). The
+ * pairs no rank or SCC test settles run 64 at a time as lanes of one search of the condensation
+ * DAG. Arrays host or device. */
+int gir_dev_reachable(gir_dev_t* g, const int32_t* u, const int32_t* v, int64_t n, uint8_t* out);
+
 /* Weight rule for edges inserted into a graph with stored weights (see apply_batch). */
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi);
 

@@ -87,6 +87,8 @@ def ref():
         R.ref_und_csr.argtypes = [_P, _P, _P]
         R.ref_und_csr.restype = _I64
         R.ref_bfs.argtypes = [_P, ctypes.c_int32, _P]
+        R.ref_reachable.argtypes = [_P, _P, _P, _I64, _P]
+        R.ref_reachable.restype = None
         R.ref_sssp.argtypes = [_P, ctypes.c_int32, ctypes.c_uint64, _P]
         R.ref_edge_weight.argtypes = [ctypes.c_int32, ctypes.c_int32]
         R.ref_edge_weight.restype = ctypes.c_uint32
@@ -341,6 +343,14 @@ class RefGIR:
         out = np.zeros(max(self.V, 1), np.int32)
         ref().ref_bfs(self.h, s, ptr(out))
         return out[:self.V]
+
+    def reachable(self, u, v):
+        """GIR::reachable for every pair (after the SCC layer is built)."""
+        u = np.ascontiguousarray(u, np.int32)
+        v = np.ascontiguousarray(v, np.int32)
+        out = np.zeros(max(len(u), 1), np.uint8)
+        ref().ref_reachable(self.h, ptr(u), ptr(v), len(u), ptr(out))
+        return out[:len(u)].astype(bool)
 
     def sssp(self, s, delta=16):
         out = np.zeros(max(self.V, 1), np.uint64)

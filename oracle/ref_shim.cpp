@@ -150,4 +150,10 @@ void ref_bct_shape(void* h, int32_t scc, int64_t* nodes, int64_t* edges) {
     delete t;
 }
 
+// GIR::reachable (gir_query.cpp:789-825) for every (u[i], v[i]).
+void ref_reachable(void* h, const int32_t* u, const int32_t* v, int64_t n, uint8_t* out) {
+    GIR* g = static_cast<GIR*>(h);
+    for (int64_t i = 0; i < n; ++i) out[i] = g->reachable(u[i], v[i]) ? 1 : 0;
+}
+
 }  // extern "C"

@@ -224,3 +224,38 @@ def test_batch_repair_plans_match_oracle(pkg, orc, s16):
     assert {"kept", "rebuilt"} <= seen["bct"], seen
     assert {"kept", "patched", "rebuilt"} <= seen["scc"], seen
     assert "patched" in seen["wcc"] or "kept" in seen["wcc"], seen
+
+
+def test_reachable_matches_reference(pkg, orc, s16):
+    """Batched reachability against the reference's own GIR::reachable (compiled from its
+    sources) and the oracle's BFS, before and after a batch: random pairs, same-SCC pairs,
+    pairs along the DAG, out-of-range ids and u == v."""
+    g, fb, fa = s16
+    d = pkg.DeviceGraph.from_graph(g)
+    d.build(pkg.native.LAYER_WCC | pkg.native.LAYER_SCC)
+    rng = np.random.default_rng(9)
+    for step in range(2):
+        cb, ca = d.csr(0)
+        scc = d.labels(pkg.native.LABEL_SCC)
+        src, dst = d.dag()
+        u = np.concatenate([rng.integers(0, g.V, 3000), src[:500], np.array([0, 5, -1, g.V])]).astype(np.int32)
+        v = np.concatenate([rng.integers(0, g.V, 3000), dst[:500], np.array([0, g.V + 3, 2, 1])]).astype(np.int32)
+        big = np.bincount(scc).argmax()
+        m = np.nonzero(scc == big)[0]
+        u = np.concatenate([u, m[:100]]).astype(np.int32)
+        v = np.concatenate([v, m[100:200]]).astype(np.int32)
+        got = d.reachable(u, v)
+        ok = (u >= 0) & (u < g.V) & (v >= 0) & (v < g.V)
+        ref = orc.RefGIR(g.V, cb.astype(np.int32), ca, *orc.transpose(g.V, cb, ca))
+        ref.build(3)
+        exp = np.zeros(len(u), bool)
+        exp[ok] = ref.reachable(u[ok], v[ok])
+        ref.close()
+        np.testing.assert_array_equal(got, exp)
+        for i in np.nonzero(ok)[0][:40]:  # a few through the oracle's BFS as well
+            assert got[i] == (orc.bfs(g.V, cb, ca, [int(u[i])])[v[i]] >= 0)
+        assert got.any() and not got.all()
+        gg = pkg.graphs.Graph(g.V, cb.astype(np.int32), ca, None, None)
+        bu, bv, bi = pkg.graphs.updates(gg, 3000, 3000, 41)
+        d.apply_batch(bu, bv, bi)
+    d.close()

@@ -204,6 +204,15 @@ bool GIR::hasUndirectedEdge(int u, int v) const {
 std::vector<int> GIR::bfs(int source) { return bfsMany({source}); }
 std::vector<uint64_t> GIR::sssp(int source, uint64_t delta) { return ssspMany({source}, delta); }
 
+bool GIR::reachable(int u, int v) { return reachableMany({u}, {v})[0] != 0; }
+
+std::vector<uint8_t> GIR::reachableMany(const std::vector<int>& u, const std::vector<int>& v) {
+    if (u.size() != v.size()) throw Error(GIR_ERR_INVALID, "reachable: u and v differ in length");
+    std::vector<uint8_t> out(u.size());
+    check(gir_dev_reachable(h_, u.data(), v.data(), (int64_t)u.size(), out.data()), "reachable");
+    return out;
+}
+
 std::vector<int> GIR::bfsMany(const std::vector<int>& sources) {
     std::vector<int> out(sources.size() * (size_t)V_);
     check(gir_dev_bfs(h_, sources.data(), (int64_t)sources.size(), out.data()), "bfs");

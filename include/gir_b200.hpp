@@ -112,6 +112,9 @@ public:
     // queries (gir.h:204-216)
     std::vector<int> bfs(int source);
     std::vector<uint64_t> sssp(int source, uint64_t delta = 16);
+    // gir.h:128-130: u ~> v (needs buildSCC_DAG); reachableMany answers a batch of pairs.
+    bool reachable(int u, int v);
+    std::vector<uint8_t> reachableMany(const std::vector<int>& u, const std::vector<int>& v);
     static uint32_t edgeWeight(int u, int v);
     // batched forms: one row of V per source
     std::vector<int> bfsMany(const std::vector<int>& sources);

@@ -46,6 +46,9 @@ int main(int argc, char** argv) {
         std::printf("bfs_0_9 %d sssp_0_1 %llu w01 %u\n", lv[9], (unsigned long long)d[1], GIR::edgeWeight(0, 1));
         std::printf("dag_rows_with_edges %d\n", count_nonempty(g.getDAG()));
         std::printf("has %d %d %d\n", g.hasDirectedEdge(2, 9), g.hasDirectedEdge(9, 2), g.hasUndirectedEdge(9, 2));
+        bool reach_ok = true;
+        for (int v = 0; v < (int)lv.size(); ++v) reach_ok = reach_ok && (g.reachable(0, v) == (lv[v] >= 0));
+        std::printf("reach_matches_bfs %d\n", (int)reach_ok);
         try {
             GIR bad("/nonexistent/dir/", "/nonexistent/dir/");
             std::printf("error_missing 0\n");

@@ -666,7 +666,7 @@ int gir_dev_destroy(gir_dev_t* g) {
     if (g->stream && g->pool) {
         store_free(g, g->fw); store_free(g, g->bw); store_free(g, g->sym);
         store_free(g, g->ws[0]); store_free(g, g->ws[1]);
-        for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->dag_rows, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
+        for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->dag_rows, &g->reach_hub, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
                           &g->cub_tmp, &g->stage_in, &g->stage_out, &g->sched_w, &g->sched_io, &g->lane_dist})
             release(g, *b);
         for (auto& b : g->scratch) release(g, b);

@@ -98,6 +98,8 @@ struct gir_dev {
     gir::DevBuf dag;                 // uint64 keys (scc_u << 32 | scc_v), sorted, distinct
     gir::DevBuf dag_rows;            // int64[V + 1]: row starts of dag by source label (reachability)
     bool dag_rows_valid = false;
+    gir::DevBuf reach_hub;           // uint64[2V]: hubs that reach v, then hubs v reaches (reachability)
+    bool reach_hub_valid = false;
     int64_t n_dag = -1;
     gir::DevBuf blk_label, blk_head, bcnt;  // int32[V], int32[n_blocks], int32[V]
     int64_t n_blocks = -1;

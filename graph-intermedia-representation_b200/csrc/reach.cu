@@ -5,12 +5,18 @@
 // whose rank lies in [rank(SCC(u)), rank(SCC(v))]; a query with rank(SCC(u)) > rank(SCC(v)) is
 // false at once. The reference answers one query by a bidirectional search over the DAG; here a
 // batch of queries is answered together:
-//  1. one kernel settles the queries that need no search (same SCC; ranks in the wrong order;
-//     ids out of range) and queues the rest;
+//  1. one kernel settles the queries that need no search and queues the rest. Besides the same
+//     SCC (true), ranks in the wrong order (false) and ids out of range, a landmark index settles
+//     most pairs: 64 hub vertices (largest out x in degree, distinct SCCs), and for every vertex
+//     F(v) = the hubs that reach v and R(v) = the hubs v reaches (two 64-lane BFS, forward and on
+//     the transposed graph, built once per condensation). Then u ~> v if R(u) & F(v) != 0 (through
+//     a hub); not if some hub reaches u but not v (F(u) & ~F(v)), or v reaches a hub u does not
+//     (R(v) & ~R(u));
 //  2. the queued ones run 64 at a time as lanes of one level-synchronous forward search over the
 //     DAG (its rows are the sorted condensation keys), every lane pruned to the SCCs whose rank is
 //     at most its target's, until every lane has reached its target or run out of frontier.
 #include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 
@@ -40,8 +46,18 @@ __global__ void k_dag_rows(const uint64_t* keys, int64_t n, int64_t V, int64_t* 
     }
 }
 
+// Masks of the landmark index from the 64 lanes' BFS levels (lane-major): bit s iff reached.
+__global__ void k_levels_to_mask(const int32_t* level, int64_t V, int nl, uint64_t* mask) {
+    GRID_STRIDE(v, V) {
+        uint64_t m = 0;
+        for (int s = 0; s < nl; ++s) m |= (uint64_t)(level[(int64_t)s * V + v] >= 0) << s;
+        mask[v] = m;
+    }
+}
+
 __global__ void k_reach_classify(const int32_t* u, const int32_t* v, int64_t n, int64_t V, const int32_t* scc,
-                                 const int32_t* rank, uint8_t* out, int32_t* pend, unsigned long long* cnt) {
+                                 const int32_t* rank, const uint64_t* F, const uint64_t* R, uint8_t* out, int32_t* pend,
+                                 unsigned long long* cnt) {
     __shared__ int32_t s_st[kBlock / 32][kStage];
     int n_st = 0;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
@@ -51,8 +67,13 @@ __global__ void k_reach_classify(const int32_t* u, const int32_t* v, int64_t n, 
             const int32_t a = u[i], b = v[i];
             uint8_t r = 0;
             if (a >= 0 && b >= 0 && a < V && b < V) {
-                if (a == b || scc[a] == scc[b]) r = 1;
-                else queue = rank[a] < rank[b];
+                if (a == b || scc[a] == scc[b]) {
+                    r = 1;
+                } else if (rank[a] < rank[b]) {
+                    const uint64_t fa = F[a], fb = F[b], ra = R[a], rb = R[b];
+                    if (ra & fb) r = 1;
+                    else queue = !((fa & ~fb) || (rb & ~ra));
+                }
             }
             out[i] = r;
         }
@@ -203,9 +224,77 @@ __global__ void k_reach_write(const int32_t* pend, int64_t g0, int nl, const uns
 
 }  // namespace
 
+// The landmark index: hubs chosen on the host from the degrees, then a 64-lane BFS from them on
+// the forward graph (F) and on the transposed graph (R, the forward and backward stores swapped
+// for the call).
+static int build_hub_index(gir_dev* g) {
+    const int64_t V = g->V;
+    uint64_t* F = nullptr;
+    GIR_TRY(ensure_n(g, g->reach_hub, 2 * (size_t)V + 1, &F));
+    uint64_t* R = F + V;
+    std::vector<int32_t> od((size_t)V), id((size_t)V), lab((size_t)V);
+    GIR_CUDA(g, cudaMemcpyAsync(od.data(), g->fw.deg, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaMemcpyAsync(id.data(), g->bw.deg, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaMemcpyAsync(lab.data(), g->scc.p, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    std::vector<std::pair<uint64_t, int32_t>> score((size_t)V);
+    for (int64_t v = 0; v < V; ++v) score[v] = {(uint64_t)(uint32_t)od[v] * (uint64_t)(uint32_t)id[v], (int32_t)v};
+    std::sort(score.begin(), score.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<int32_t> hubs;
+    std::vector<int32_t> used;
+    for (const auto& sv : score) {
+        if ((int)hubs.size() == 64 || sv.first == 0) break;
+        const int32_t l = lab[sv.second];
+        if (std::find(used.begin(), used.end(), l) != used.end()) continue;
+        used.push_back(l);
+        hubs.push_back(sv.second);
+    }
+    const int nl = (int)hubs.size();
+    if (nl == 0) {
+        GIR_CUDA(g, cudaMemsetAsync(F, 0, sizeof(uint64_t) * 2 * V, g->stream));
+        g->reach_hub_valid = true;
+        return GIR_OK;
+    }
+    int32_t *hubs_d = nullptr, *level = nullptr;
+    GIR_TRY(dev_alloc_n(g, &hubs_d, 64));
+    GIR_TRY(dev_alloc_n(g, &level, (size_t)nl * V + 1));
+    GIR_CUDA(g, cudaMemcpyAsync(hubs_d, hubs.data(), sizeof(int32_t) * nl, cudaMemcpyHostToDevice, g->stream));
+    std::vector<int64_t> sb((size_t)nl + 1);
+    for (int i = 0; i <= nl; ++i) sb[i] = i;
+    const QueryStats keep = g->qstats;
+    const int sched = g->schedule;
+    g->schedule = GIR_SCHEDULE_FIXED;
+    int rc = bfs_run(g, sb.data(), hubs_d, nl, level);
+    if (rc == GIR_OK) {
+        k_levels_to_mask<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(level, V, nl, F);
+        rc = cuda_check(g, cudaGetLastError(), "k_levels_to_mask");
+    }
+    if (rc == GIR_OK) {  // the transposed graph: swap the two stores around one more BFS
+        std::swap(g->fw, g->bw);
+        g->bins_valid = false;
+        rc = bfs_run(g, sb.data(), hubs_d, nl, level);
+        std::swap(g->fw, g->bw);
+        g->bins_valid = false;
+        if (rc == GIR_OK) {
+            k_levels_to_mask<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(level, V, nl, R);
+            rc = cuda_check(g, cudaGetLastError(), "k_levels_to_mask");
+        }
+    }
+    g->schedule = sched;
+    g->qstats = keep;
+    dev_free(g, level);
+    dev_free(g, hubs_d);
+    GIR_TRY(rc);
+    g->reach_hub_valid = true;
+    return GIR_OK;
+}
+
 int reach_run(gir_dev* g, const int32_t* u_d, const int32_t* v_d, int64_t n, uint8_t* out_d) {
     const int64_t V = g->V;
     if (n <= 0) return GIR_OK;
+    if (!g->reach_hub_valid) GIR_TRY(build_hub_index(g));
+    const uint64_t* hubF = static_cast<const uint64_t*>(g->reach_hub.p);
+    const uint64_t* hubR = hubF + V;
     const int32_t* scc = static_cast<const int32_t*>(g->scc.p);
     const int32_t* rank = static_cast<const int32_t*>(g->scc_rank.p);
     const uint64_t* keys = static_cast<const uint64_t*>(g->dag.p);
@@ -240,7 +329,8 @@ int reach_run(gir_dev* g, const int32_t* u_d, const int32_t* v_d, int64_t n, uin
         return GIR_OK;
     };
     GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * R_N, g->stream));
-    k_reach_classify<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(u_d, v_d, n, V, scc, rank, out_d, pend, cnt);
+    k_reach_classify<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(u_d, v_d, n, V, scc, rank, hubF, hubR, out_d,
+                                                                       pend, cnt);
     GIR_LAUNCH(g, "k_reach_classify");
     GIR_TRY(read());
     const int64_t n_pend = (int64_t)hc[R_Q];

@@ -467,6 +467,7 @@ int scc_build_dag(gir_dev* g) {
     }
     g->n_dag = n_dag;
     g->dag_rows_valid = false;
+    g->reach_hub_valid = false;
     trace_mark(g, "scc: dag edges");
 
     // topological ranks: longest-path levels over the condensation edges, rounds until stable

@@ -436,6 +436,18 @@ class GIR:
         """gir.h:128-130 (gir_query.cpp:789-825); batches go through DeviceGraph.reachable."""
         return bool(self._d.reachable([u], [v])[0])
 
+    # gir.h:208-216: the reference's task-parallel formulations of the same queries (a wavefront
+    # over the condensation DAG with block tasks inside SCCs) return what bfs / sssp return; on
+    # the device the flat lane-parallel traversal is that computation.
+    def bfsTwoLevel(self, source):
+        return self.bfs(source)
+
+    def bfsTaskParallel(self, source):
+        return self.bfs(source)
+
+    def ssspTwoLevel(self, source, delta=16):
+        return self.sssp(source, delta)
+
     @staticmethod
     def edgeWeight(u, v):
         """gir_query.cpp:50-54 (computed on the host here only to answer this static call)."""

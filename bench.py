@@ -551,6 +551,10 @@ def run_ours(args):
         rout = torch.empty(n_r, dtype=torch.uint8, device=dev)
         d.reachable(ru[:64], rv[:64], out=rout[:64])
         t_r = ev_time(stream, lambda: d.reachable(ru, rv, out=rout))
+        # betweenness (GIR::bc) over the step's 64 BFS sources
+        bc_out = torch.empty(V, dtype=torch.float64, device=dev)
+        t_bc = ev_time(stream, lambda: d.bc(sb_d, out=bc_out))
+        extra["bc_64_sources_ms"] = t_bc
         extra["reachable"] = {"pairs": n_r, "ms": t_r, "pairs_per_s": n_r / (t_r * 1e-3),
                               "true_fraction": float(rout.float().mean().item())}
         if rep is not None:

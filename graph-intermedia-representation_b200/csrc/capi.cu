@@ -853,6 +853,22 @@ int gir_dev_autotune(gir_dev_t* g, const int32_t* srcs, int64_t n_src, int reps,
     return GIR_OK;
 }
 
+int gir_dev_bc(gir_dev_t* g, const int32_t* srcs, int64_t n_src, double* score_out) {
+    if (!g) return GIR_ERR_INVALID;
+    if (n_src < 0 || !score_out || (n_src > 0 && !srcs)) return fail(g, GIR_ERR_INVALID, "bc: bad arguments");
+    DevBuf ss;
+    const void* ds = nullptr;
+    void* dout = nullptr;
+    int rc = GIR_OK;
+    if (!(rc = stage_input(g, ss, srcs, sizeof(int32_t) * n_src, &ds)) &&
+        !(rc = out_target(g, score_out, sizeof(double) * (size_t)g->V, g->stage_out, &dout)) &&
+        !(rc = bc_run(g, (const int32_t*)ds, n_src, (double*)dout)))
+        rc = finish_out(g, score_out, dout, sizeof(double) * (size_t)g->V);
+    release(g, ss);
+    release_scratch(g, kKeepScratchBelow);
+    return rc;
+}
+
 int gir_dev_reachable(gir_dev_t* g, const int32_t* u, const int32_t* v, int64_t n, uint8_t* out) {
     if (!g) return GIR_ERR_INVALID;
     if (n < 0 || (n > 0 && (!u || !v || !out))) return fail(g, GIR_ERR_INVALID, "reachable: bad arguments");

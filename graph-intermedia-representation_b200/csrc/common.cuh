@@ -256,6 +256,8 @@ int wcc_union_pairs(gir_dev* g, const uint64_t* keys, int64_t n);
 int scc_build(gir_dev* g);
 // Condensation DAG and ranks from the current SCC labels (the labels are kept).
 int scc_build_dag(gir_dev* g);
+// Betweenness of every vertex over the sources (device arrays; score has V entries).
+int bc_run(gir_dev* g, const int32_t* srcs_d, int64_t n_src, double* score_d);
 // Reachability of every pair (u[i], v[i]) into out[i] (device arrays; the SCC layer is built).
 int reach_run(gir_dev* g, const int32_t* u_d, const int32_t* v_d, int64_t n, uint8_t* out_d);
 int bct_build(gir_dev* g);

@@ -204,6 +204,13 @@ class DeviceGraph:
         self._ck(dev_lib().gir_dev_reachable(self._h, ptr(su), ptr(sv), n, ptr(res)), "reachable")
         return res.astype(bool) if out is None else res
 
+    def bc(self, sources, out=None):
+        """GIR::bc: betweenness of every vertex over `sources` (float64[V], or fills `out`)."""
+        s, n = self._ids(sources)
+        res = np.empty(self.V, np.float64) if out is None else out
+        self._ck(dev_lib().gir_dev_bc(self._h, ptr(s), n, ptr(res)), "bc")
+        return res
+
     def batch_plan(self):
         """Per layer, what the last batch did: 'kept', 'patched' or 'rebuilt'."""
         out = np.zeros(3, np.int32)
@@ -439,6 +446,10 @@ class GIR:
     # gir.h:208-216: the reference's task-parallel formulations of the same queries (a wavefront
     # over the condensation DAG with block tasks inside SCCs) return what bfs / sssp return; on
     # the device the flat lane-parallel traversal is that computation.
+    def bc(self, sources):
+        """gir.h:217-219 (gir_query.cpp:728-778)."""
+        return self._d.bc(sources)
+
     def bfsTwoLevel(self, source):
         return self.bfs(source)
 

@@ -34,7 +34,7 @@ DEV_SYMBOLS = (
     "gir_dev_get_param", "gir_dev_query_stats", "gir_dev_stream", "gir_dev_sched_set_weights",
     "gir_dev_sched_get_weights", "gir_dev_sched_param_count", "gir_dev_sched_train", "gir_dev_sched_forward",
     "gir_dev_sched_grad", "gir_dev_bfs_noalloc", "gir_dev_sched_trace", "gir_dev_sched_delta_choices",
-    "gir_dev_batch_times", "gir_dev_batch_plan", "gir_dev_autotune", "gir_dev_reachable",
+    "gir_dev_batch_times", "gir_dev_batch_plan", "gir_dev_autotune", "gir_dev_reachable", "gir_dev_bc",
 )
 GEN_SYMBOLS = (
     "gir_gen_last_error", "gir_gen_free", "gir_gen_hash3", "gir_gen_rmat", "gir_gen_lattice", "gir_gen_csr",
@@ -109,6 +109,7 @@ def dev_lib():
             "gir_dev_batch_plan": [_P, _P],
             "gir_dev_autotune": [_P, _P, _I64, ctypes.c_int, ctypes.POINTER(ctypes.c_double)],
             "gir_dev_reachable": [_P, _P, _P, _I64, _P],
+            "gir_dev_bc": [_P, _P, _I64, _P],
         }
         for name, args in sig.items():
             f = getattr(lib, name)

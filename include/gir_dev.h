@@ -176,6 +176,11 @@ int gir_dev_autotune(gir_dev_t* g, const int32_t* srcs, int64_t n_src, int reps,
  * DAG. Arrays host or device. */
 int gir_dev_reachable(gir_dev_t* g, const int32_t* u, const int32_t* v, int64_t n, uint8_t* out);
 
+/* GIR::bc (gir_query.cpp:728-778): Brandes betweenness on the directed graph, unweighted,
+ * score_out[v] = sum over the n_src sources s != v of delta_s(v) (V doubles; sources repeat as
+ * given, ids out of range add nothing). 64 sources share one traversal. */
+int gir_dev_bc(gir_dev_t* g, const int32_t* srcs, int64_t n_src, double* score_out);
+
 /* Weight rule for edges inserted into a graph with stored weights (see apply_batch). */
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi);
 

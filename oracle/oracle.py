@@ -88,6 +88,8 @@ def ref():
         R.ref_und_csr.restype = _I64
         R.ref_bfs.argtypes = [_P, ctypes.c_int32, _P]
         R.ref_reachable.argtypes = [_P, _P, _P, _I64, _P]
+        R.ref_bc.argtypes = [_P, _P, _I64, _P]
+        R.ref_bc.restype = None
         R.ref_reachable.restype = None
         R.ref_sssp.argtypes = [_P, ctypes.c_int32, ctypes.c_uint64, _P]
         R.ref_edge_weight.argtypes = [ctypes.c_int32, ctypes.c_int32]
@@ -342,6 +344,13 @@ class RefGIR:
     def bfs(self, s):
         out = np.zeros(max(self.V, 1), np.int32)
         ref().ref_bfs(self.h, s, ptr(out))
+        return out[:self.V]
+
+    def bc(self, sources):
+        """GIR::bc over the sources (float64[V])."""
+        s = np.ascontiguousarray(sources, np.int32)
+        out = np.zeros(max(self.V, 1), np.float64)
+        ref().ref_bc(self.h, ptr(s), len(s), ptr(out))
         return out[:self.V]
 
     def reachable(self, u, v):

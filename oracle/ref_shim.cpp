@@ -156,4 +156,11 @@ void ref_reachable(void* h, const int32_t* u, const int32_t* v, int64_t n, uint8
     for (int64_t i = 0; i < n; ++i) out[i] = g->reachable(u[i], v[i]) ? 1 : 0;
 }
 
+// GIR::bc (gir_query.cpp:728-778) into score[V].
+void ref_bc(void* h, const int32_t* src, int64_t n, double* score) {
+    GIR* g = static_cast<GIR*>(h);
+    auto r = g->bc(std::vector<int>(src, src + n));
+    for (int v = 0; v < g->vertexCount(); ++v) score[v] = r[v];
+}
+
 }  // extern "C"

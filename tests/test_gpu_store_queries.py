@@ -266,3 +266,21 @@ def test_persistent_levels_on_a_lattice(pkg, orc):
         for i, s in enumerate(sets):
             np.testing.assert_array_equal(ls[i], orc.bfs(lat.V, fb, fa, list(s)))
     d.close()
+
+
+def test_betweenness_matches_reference(pkg, orc, s16):
+    """Brandes betweenness (GIR::bc) against the reference's own implementation: two graphs, more
+    sources than one 64-lane group, repeated and out-of-range sources. Doubles: the sums run in
+    another order than the reference's, so the bar is a relative 1e-9."""
+    small = pkg.graphs.rmat(12, seed=14, weights=None)
+    g, _, _ = s16
+    for gr, n in ((small, 70), (g, 100)):
+        d = pkg.DeviceGraph.from_graph(gr, weights=False)
+        src = np.concatenate([pkg.graphs.sources_with_edges(gr, n, 3), [0, 0, -5, gr.V + 2]]).astype(np.int32)
+        got = d.bc(src)
+        ref = orc.RefGIR(gr.V, gr.fw_beg, gr.fw_adj, gr.bw_beg, gr.bw_adj)
+        exp = ref.bc(src)
+        ref.close()
+        np.testing.assert_allclose(got, exp, rtol=1e-9, atol=1e-9)
+        assert exp.max() > 0
+        d.close()

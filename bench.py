@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-schedule", action="store_true", help="skip the learned-vs-fixed schedule comparison")
     p.add_argument("--no-batched", action="store_true", help="skip the batched queries + uneven batches section")
+    p.add_argument("--no-incremental", action="store_true", help="skip the incremental BFS / SSSP section")
     p.add_argument("--stream", type=int, default=0, metavar="ROUNDS",
                    help="instead of the bench: the 41.6M-vertex / 1.47B-edge R-MAT (seed 5, weights U[1,1023]), "
                         "WCC + SCC build, then ROUNDS x (1M-edge batch 60/40 + 32 BFS + 32 SSSP), checked by "
@@ -255,6 +256,82 @@ def run_reference(args):
             "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def incremental_section(pkg, d, stream, dev, src, with_ref):
+    """Incremental single-source BFS / SSSP (GIR::trackIncremental / updateIncremental) on the
+    current graph: batches of 1K / 10K / 100K ops (two thirds deletions of existing edges, one third
+    random insertions), each applied (untimed here) and followed by the update of both tracked
+    results, timed against a from-scratch query of the same source; after every update both results
+    must equal the from-scratch ones. With with_ref the reference (compiled from its sources) tracks
+    the same source and takes the same batches (ingestBatch); its updateIncremental is timed on the
+    host cores beside the device's and its results must equal the device's."""
+    import numpy as np
+    import torch
+    V = d.V
+    rng = np.random.default_rng(123)
+    s_d = torch.tensor([src], dtype=torch.int32, device=dev)
+    ds1 = torch.empty((1, V), dtype=torch.int64, device=dev)
+    lv1 = torch.empty((1, V), dtype=torch.int32, device=dev)
+    inc = torch.empty(V, dtype=torch.int64, device=dev)
+    d.sssp(s_d, delta=DELTA, out=ds1)  # warm
+    res = {"source": src, "scratch_ms": {"sssp": ev_time(stream, lambda: d.sssp(s_d, delta=DELTA, out=ds1)),
+                                         "bfs": ev_time(stream, lambda: d.bfs(s_d, out=lv1))},
+           "track_ms": {"sssp": ev_time(stream, lambda: d.inc_track(src, True)),
+                        "bfs": ev_time(stream, lambda: d.inc_track(src, False))}, "batches": {}}
+    cb, ca = d.csr(0)
+    ref = None
+    if with_ref:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        if oracle.ref_available():
+            bb, ba = d.csr(1)
+            ref = oracle.RefGIR(V, cb.astype(np.int32), ca, bb.astype(np.int32), ba)
+            t = time.perf_counter()
+            ref.inc_track(src, True)
+            ref.inc_track(src, False)
+            res["ref_track_s"] = time.perf_counter() - t
+            res["ref_threads"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    none = np.iinfo(np.uint64).max
+    for k in (1_000, 10_000, 100_000):
+        a = rng.integers(0, V, 2 * k // 3)
+        a = a[cb[a + 1] > cb[a]]
+        b = ca[cb[a] + rng.integers(0, 1 << 30, len(a)) % (cb[a + 1] - cb[a])]
+        n_ins = k - len(a)
+        u = np.concatenate([a, rng.integers(0, V, n_ins)]).astype(np.int32)
+        v = np.concatenate([b, rng.integers(0, V, n_ins)]).astype(np.int32)
+        ins = np.concatenate([np.zeros(len(a)), np.ones(n_ins)]).astype(np.uint8)
+        d.apply_batch(u, v, ins)
+        row = {"ops": k, "sssp_update_ms": ev_time(stream, lambda: d.inc_update(True))}
+        st = d.query_stats()
+        row.update(cut_vertices=st["reached"], rounds=st["iterations"], relaxed_entries=st["edges"])
+        row["bfs_update_ms"] = ev_time(stream, lambda: d.inc_update(False))
+        d.sssp(s_d, delta=DELTA, out=ds1)
+        d.inc_dist(True, out=inc)
+        ok_w = bool(torch.equal(inc, ds1[0]))
+        d.bfs(s_d, out=lv1)
+        d.inc_dist(False, out=inc)
+        lv = lv1[0].to(torch.int64)
+        ok_b = bool(torch.equal(inc, torch.where(lv < 0, torch.full_like(lv, -1), lv)))
+        row["identical_to_scratch"] = ok_w and ok_b
+        if ref is not None:
+            ref.ingest_batch(u, v, ins)
+            t = time.perf_counter()
+            ref.inc_update(True)
+            row["ref_sssp_update_ms"] = (time.perf_counter() - t) * 1e3
+            t = time.perf_counter()
+            ref.inc_update(False)
+            row["ref_bfs_update_ms"] = (time.perf_counter() - t) * 1e3
+            dw = d.inc_dist(True)
+            db = d.inc_dist(False)
+            row["identical_to_reference"] = bool(np.array_equal(dw, ref.inc_dist(True)) and
+                                                 np.array_equal(db, ref.inc_dist(False)))
+            assert dw[src] == 0 and db[src] == 0 and (dw != none).sum() == (db != none).sum()
+        res["batches"][str(k)] = row
+        cb, ca = d.csr(0)
+    if ref is not None:
+        ref.close()
+    return res
 
 
 def ev_time(stream, fn):
@@ -555,6 +632,10 @@ def run_ours(args):
         bc_out = torch.empty(V, dtype=torch.float64, device=dev)
         t_bc = ev_time(stream, lambda: d.bc(sb_d, out=bc_out))
         extra["bc_64_sources_ms"] = t_bc
+        # incremental BFS / SSSP of one source under 1K / 10K / 100K-op batches
+        if not args.no_incremental:
+            extra["incremental"] = incremental_section(pkg, d, stream, dev, int(sb_d[0].item()),
+                                                       rank == 0 and world == 1 and not args.no_cpu)
         extra["reachable"] = {"pairs": n_r, "ms": t_r, "pairs_per_s": n_r / (t_r * 1e-3),
                               "true_fraction": float(rout.float().mean().item())}
         if rep is not None:

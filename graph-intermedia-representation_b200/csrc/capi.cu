@@ -447,6 +447,7 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     g->b_ins = n_ins;
     g->b_del = n_del;
     if (n_ins + n_del == 0) return GIR_OK;
+    GIR_TRY(inc_log(g, ins_k, n_ins, del_k, n_del));
     trace_mark(g, "batch: normalize");
     if (g->scc_built) {
         k_classify_directed<<<grid_for(g, n_ins + n_del, kBlock), kBlock, 0, g->stream>>>(
@@ -667,7 +668,8 @@ int gir_dev_destroy(gir_dev_t* g) {
         store_free(g, g->fw); store_free(g, g->bw); store_free(g, g->sym);
         store_free(g, g->ws[0]); store_free(g, g->ws[1]);
         for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->dag_rows, &g->reach_hub, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
-                          &g->cub_tmp, &g->stage_in, &g->stage_out, &g->sched_w, &g->sched_io, &g->lane_dist})
+                          &g->cub_tmp, &g->stage_in, &g->stage_out, &g->sched_w, &g->sched_io, &g->lane_dist, &g->inc_st[0], &g->inc_st[1],
+                          &g->inc_pend[0], &g->inc_pend[1]})
             release(g, *b);
         for (auto& b : g->scratch) release(g, b);
         for (auto& b : g->work) release(g, b);
@@ -867,6 +869,29 @@ int gir_dev_bc(gir_dev_t* g, const int32_t* srcs, int64_t n_src, double* score_o
     release(g, ss);
     release_scratch(g, kKeepScratchBelow);
     return rc;
+}
+
+int gir_dev_inc_track(gir_dev_t* g, int32_t source, int weighted) {
+    if (!g) return GIR_ERR_INVALID;
+    const int rc = inc_track(g, source, weighted ? 1 : 0);
+    release_scratch(g, kKeepScratchBelow);
+    return rc;
+}
+
+int gir_dev_inc_update(gir_dev_t* g, int weighted) {
+    if (!g) return GIR_ERR_INVALID;
+    return inc_update(g, weighted ? 1 : 0);
+}
+
+int gir_dev_inc_dist(gir_dev_t* g, int weighted, uint64_t* dist_out) {
+    if (!g) return GIR_ERR_INVALID;
+    if (!dist_out) return fail(g, GIR_ERR_INVALID, "inc_dist: bad arguments");
+    if (!g->inc_on[weighted ? 1 : 0]) return fail(g, GIR_ERR_STATE, "inc_dist: the mode is not tracked");
+    void* dout = nullptr;
+    const size_t bytes = sizeof(uint64_t) * (size_t)g->V;
+    GIR_TRY(out_target(g, dist_out, bytes, g->stage_out, &dout));
+    GIR_TRY(inc_dist(g, weighted ? 1 : 0, static_cast<uint64_t*>(dout)));
+    return finish_out(g, dist_out, dout, bytes);
 }
 
 int gir_dev_reachable(gir_dev_t* g, const int32_t* u, const int32_t* v, int64_t n, uint8_t* out) {

@@ -104,6 +104,14 @@ struct gir_dev {
     gir::DevBuf blk_label, blk_head, bcnt;  // int32[V], int32[n_blocks], int32[V]
     int64_t n_blocks = -1;
 
+    // Incremental single-source results ([0] BFS, [1] SSSP with the hash weights): per vertex
+    // dist << 32 | parent (all ones = unreachable), and the edge keys (u << 32 | v) changed by
+    // batches since the last update.
+    bool inc_on[2] = {false, false};
+    int32_t inc_src[2] = {-1, -1};
+    gir::DevBuf inc_st[2], inc_pend[2];
+    int64_t inc_npend[2] = {0, 0};
+
     // Weight-sorted copies of the forward CSR for SSSP ([0] hash weights, [1] stored weights).
     gir::DevCSR ws[2];
     bool ws_valid[2] = {false, false};
@@ -261,6 +269,12 @@ int bc_run(gir_dev* g, const int32_t* srcs_d, int64_t n_src, double* score_d);
 // Reachability of every pair (u[i], v[i]) into out[i] (device arrays; the SCC layer is built).
 int reach_run(gir_dev* g, const int32_t* u_d, const int32_t* v_d, int64_t n, uint8_t* out_d);
 int bct_build(gir_dev* g);
+// Incremental BFS / SSSP (incr.cu): track one source, log a batch's changed edges (device keys),
+// correct the tracked result for the logged changes, and write its distances (device, V entries).
+int inc_track(gir_dev* g, int32_t source, int weighted);
+int inc_log(gir_dev* g, const uint64_t* ins, int64_t n_ins, const uint64_t* del, int64_t n_del);
+int inc_update(gir_dev* g, int weighted);
+int inc_dist(gir_dev* g, int weighted, uint64_t* out_d);
 
 // ---- queries ----
 int bfs_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t n_sets, int32_t* level_d);

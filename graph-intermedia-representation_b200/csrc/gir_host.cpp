@@ -213,6 +213,26 @@ std::vector<uint8_t> GIR::reachableMany(const std::vector<int>& u, const std::ve
     return out;
 }
 
+void GIR::trackIncremental(int source, bool weighted) {
+    check(gir_dev_inc_track(h_, source, weighted ? 1 : 0), "trackIncremental");
+    inc_[weighted].clear();
+}
+
+void GIR::updateIncremental(bool weighted) {
+    check(gir_dev_inc_update(h_, weighted ? 1 : 0), "updateIncremental");
+    inc_[weighted].clear();
+}
+
+uint64_t GIR::incDist(bool weighted, int v) const {
+    std::vector<uint64_t>& c = inc_[weighted];
+    if (c.empty() && V_ > 0) {
+        c.resize((size_t)V_);
+        check(gir_dev_inc_dist(h_, weighted ? 1 : 0, c.data()), "incDist");
+    }
+    if (v < 0 || v >= V_) throw Error(GIR_ERR_INVALID, "incDist: vertex out of range");
+    return c[(size_t)v];
+}
+
 std::vector<int> GIR::bfsMany(const std::vector<int>& sources) {
     std::vector<int> out(sources.size() * (size_t)V_);
     check(gir_dev_bfs(h_, sources.data(), (int64_t)sources.size(), out.data()), "bfs");

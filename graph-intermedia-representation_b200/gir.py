@@ -211,6 +211,21 @@ class DeviceGraph:
         self._ck(dev_lib().gir_dev_bc(self._h, ptr(s), n, ptr(res)), "bc")
         return res
 
+    def inc_track(self, source, weighted):
+        """GIR::trackIncremental: BFS (weighted False) or SSSP (True, GIR::edgeWeight) of one
+        source, kept up to date by inc_update under later batches."""
+        self._ck(dev_lib().gir_dev_inc_track(self._h, int(source), 1 if weighted else 0), "inc_track")
+
+    def inc_update(self, weighted):
+        """GIR::updateIncremental: corrects the tracked result for the edges changed since."""
+        self._ck(dev_lib().gir_dev_inc_update(self._h, 1 if weighted else 0), "inc_update")
+
+    def inc_dist(self, weighted, out=None):
+        """The tracked levels / distances of every vertex (uint64[V], UINT64_MAX = unreachable)."""
+        res = np.empty(self.V, np.uint64) if out is None else out
+        self._ck(dev_lib().gir_dev_inc_dist(self._h, 1 if weighted else 0, ptr(res)), "inc_dist")
+        return res
+
     def batch_plan(self):
         """Per layer, what the last batch did: 'kept', 'patched' or 'rebuilt'."""
         out = np.zeros(3, np.int32)
@@ -315,6 +330,7 @@ class GIR:
         else:
             self._d = DeviceGraph.load(path_directed)  # GIR(dir, und_dir) (gir.h:93)
         self._V = self._d.V
+        self._inc = {False: None, True: None}
 
     @property
     def device(self):
@@ -449,6 +465,22 @@ class GIR:
     def bc(self, sources):
         """gir.h:217-219 (gir_query.cpp:728-778)."""
         return self._d.bc(sources)
+
+    # gir.h:220-232 (gir_query.cpp:867-996). incDist reads a host copy of the tracked result,
+    # taken after each track / update (the result changes only there).
+    def trackIncremental(self, source, weighted):
+        self._d.inc_track(source, weighted)
+        self._inc[bool(weighted)] = None
+
+    def updateIncremental(self, weighted):
+        self._d.inc_update(weighted)
+        self._inc[bool(weighted)] = None
+
+    def incDist(self, weighted, v):
+        w = bool(weighted)
+        if self._inc[w] is None:
+            self._inc[w] = self._d.inc_dist(w)
+        return int(self._inc[w][v])
 
     def bfsTwoLevel(self, source):
         return self.bfs(source)

@@ -35,6 +35,7 @@ DEV_SYMBOLS = (
     "gir_dev_sched_get_weights", "gir_dev_sched_param_count", "gir_dev_sched_train", "gir_dev_sched_forward",
     "gir_dev_sched_grad", "gir_dev_bfs_noalloc", "gir_dev_sched_trace", "gir_dev_sched_delta_choices",
     "gir_dev_batch_times", "gir_dev_batch_plan", "gir_dev_autotune", "gir_dev_reachable", "gir_dev_bc",
+    "gir_dev_inc_track", "gir_dev_inc_update", "gir_dev_inc_dist",
 )
 GEN_SYMBOLS = (
     "gir_gen_last_error", "gir_gen_free", "gir_gen_hash3", "gir_gen_rmat", "gir_gen_lattice", "gir_gen_csr",
@@ -110,6 +111,9 @@ def dev_lib():
             "gir_dev_autotune": [_P, _P, _I64, ctypes.c_int, ctypes.POINTER(ctypes.c_double)],
             "gir_dev_reachable": [_P, _P, _P, _I64, _P],
             "gir_dev_bc": [_P, _P, _I64, _P],
+            "gir_dev_inc_track": [_P, _I32, ctypes.c_int],
+            "gir_dev_inc_update": [_P, ctypes.c_int],
+            "gir_dev_inc_dist": [_P, ctypes.c_int, _P],
         }
         for name, args in sig.items():
             f = getattr(lib, name)

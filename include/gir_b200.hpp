@@ -116,6 +116,12 @@ public:
     bool reachable(int u, int v);
     std::vector<uint8_t> reachableMany(const std::vector<int>& u, const std::vector<int>& v);
     static uint32_t edgeWeight(int u, int v);
+    // gir.h:220-232 (gir_query.cpp:867-996): incremental single-source BFS (weighted false) /
+    // SSSP (true). incDist reads a host copy of the tracked result, taken after each track or
+    // update (the result changes only there).
+    void trackIncremental(int source, bool weighted);
+    void updateIncremental(bool weighted);
+    uint64_t incDist(bool weighted, int v) const;
     // batched forms: one row of V per source
     std::vector<int> bfsMany(const std::vector<int>& sources);
     std::vector<uint64_t> ssspMany(const std::vector<int>& sources, uint64_t delta = 16);
@@ -130,6 +136,7 @@ private:
 
     gir_dev_t* h_ = nullptr;
     int V_ = 0;
+    mutable std::vector<uint64_t> inc_[2];  // host copies of the tracked results (empty = stale)
 };
 
 }  // namespace gir_b200

@@ -181,6 +181,21 @@ int gir_dev_reachable(gir_dev_t* g, const int32_t* u, const int32_t* v, int64_t 
  * given, ids out of range add nothing). 64 sources share one traversal. */
 int gir_dev_bc(gir_dev_t* g, const int32_t* srcs, int64_t n_src, double* score_out);
 
+/* Incremental single-source BFS (weighted = 0) / SSSP (weighted = 1, GIR::edgeWeight weights),
+ * KickStarter-style: gir_dev_inc_track replaces GIR::trackIncremental (gir_query.cpp:867-892):
+ * it computes the source's result and its dependence tree, and from then on every edge a batch
+ * changes is logged for that mode. gir_dev_inc_update replaces GIR::updateIncremental
+ * (gir_query.cpp:894-996): it corrects the result for the logged changes (nothing to do when the
+ * mode is untracked, its source is negative or nothing was logged). gir_dev_inc_dist replaces
+ * GIR::incDist (gir.h:229-232) for every vertex at once: dist_out[v] (V entries, host or device)
+ * = the level / distance of v, UINT64_MAX = unreachable; GIR_ERR_STATE when the mode was never
+ * tracked. A source out of range tracks an all-unreachable result, as GIR::bfs / sssp give one.
+ * After an update, gir_dev_query_stats gives: iterations = propagation rounds, reached = vertices
+ * whose tree edge was cut (and their subtrees), edges = frontier entries relaxed. */
+int gir_dev_inc_track(gir_dev_t* g, int32_t source, int weighted);
+int gir_dev_inc_update(gir_dev_t* g, int weighted);
+int gir_dev_inc_dist(gir_dev_t* g, int weighted, uint64_t* dist_out);
+
 /* Weight rule for edges inserted into a graph with stored weights (see apply_batch). */
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi);
 

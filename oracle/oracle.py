@@ -90,6 +90,14 @@ def ref():
         R.ref_reachable.argtypes = [_P, _P, _P, _I64, _P]
         R.ref_bc.argtypes = [_P, _P, _I64, _P]
         R.ref_bc.restype = None
+        R.ref_ingest_batch.argtypes = [_P, _P, _P, _P, _I64]
+        R.ref_ingest_batch.restype = None
+        R.ref_inc_track.argtypes = [_P, ctypes.c_int32, ctypes.c_int]
+        R.ref_inc_track.restype = None
+        R.ref_inc_update.argtypes = [_P, ctypes.c_int]
+        R.ref_inc_update.restype = None
+        R.ref_inc_dist.argtypes = [_P, ctypes.c_int, _P]
+        R.ref_inc_dist.restype = None
         R.ref_reachable.restype = None
         R.ref_sssp.argtypes = [_P, ctypes.c_int32, ctypes.c_uint64, _P]
         R.ref_edge_weight.argtypes = [ctypes.c_int32, ctypes.c_int32]
@@ -353,6 +361,20 @@ class RefGIR:
         ref().ref_bc(self.h, ptr(s), len(s), ptr(out))
         return out[:self.V]
 
+    def inc_track(self, source, weighted):
+        """GIR::trackIncremental."""
+        ref().ref_inc_track(self.h, int(source), 1 if weighted else 0)
+
+    def inc_update(self, weighted):
+        """GIR::updateIncremental."""
+        ref().ref_inc_update(self.h, 1 if weighted else 0)
+
+    def inc_dist(self, weighted):
+        """GIR::incDist of every vertex (uint64[V])."""
+        out = np.zeros(max(self.V, 1), np.uint64)
+        ref().ref_inc_dist(self.h, 1 if weighted else 0, ptr(out))
+        return out[:self.V]
+
     def reachable(self, u, v):
         """GIR::reachable for every pair (after the SCC layer is built)."""
         u = np.ascontiguousarray(u, np.int32)
@@ -371,6 +393,13 @@ class RefGIR:
         v = np.ascontiguousarray(v, np.int32)
         ins = np.ascontiguousarray(ins, np.uint8)
         ref().ref_apply_batch(self.h, ptr(u), ptr(v), ptr(ins), len(u))
+
+    def ingest_batch(self, u, v, ins):
+        """GIR::ingestBatch: edge store and incremental logs only (layers wait for sync)."""
+        u = np.ascontiguousarray(u, np.int32)
+        v = np.ascontiguousarray(v, np.int32)
+        ins = np.ascontiguousarray(ins, np.uint8)
+        ref().ref_ingest_batch(self.h, ptr(u), ptr(v), ptr(ins), len(u))
 
     def update_edge(self, u, v, insert, undirected=False):
         ref().ref_update_edge(self.h, u, v, int(insert), int(undirected))

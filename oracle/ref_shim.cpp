@@ -91,6 +91,14 @@ void ref_apply_batch(void* h, const int32_t* u, const int32_t* v, const uint8_t*
     static_cast<GIR*>(h)->applyBatch(b);
 }
 
+// GIR::ingestBatch (gir.cpp:3588-3596): the edge store and the incremental logs only; the layers
+// wait for sync().
+void ref_ingest_batch(void* h, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n) {
+    std::vector<GIR::Update> b(n);
+    for (int64_t i = 0; i < n; ++i) b[i] = {u[i], v[i], ins[i] != 0};
+    static_cast<GIR*>(h)->ingestBatch(b);
+}
+
 void ref_update_edge(void* h, int32_t u, int32_t v, int insert, int undirected) {
     GIR* g = static_cast<GIR*>(h);
     if (undirected) g->updateEdgeUndirected(u, v, insert != 0);
@@ -161,6 +169,17 @@ void ref_bc(void* h, const int32_t* src, int64_t n, double* score) {
     GIR* g = static_cast<GIR*>(h);
     auto r = g->bc(std::vector<int>(src, src + n));
     for (int v = 0; v < g->vertexCount(); ++v) score[v] = r[v];
+}
+
+// GIR::trackIncremental / updateIncremental (gir_query.cpp:867-996) and GIR::incDist (gir.h:229-232)
+// for every vertex into dist[V].
+void ref_inc_track(void* h, int32_t src, int weighted) { static_cast<GIR*>(h)->trackIncremental(src, weighted != 0); }
+
+void ref_inc_update(void* h, int weighted) { static_cast<GIR*>(h)->updateIncremental(weighted != 0); }
+
+void ref_inc_dist(void* h, int weighted, uint64_t* dist) {
+    GIR* g = static_cast<GIR*>(h);
+    for (int v = 0; v < g->vertexCount(); ++v) dist[v] = g->incDist(weighted != 0, v);
 }
 
 }  // extern "C"

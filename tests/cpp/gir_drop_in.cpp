@@ -49,6 +49,22 @@ int main(int argc, char** argv) {
         bool reach_ok = true;
         for (int v = 0; v < (int)lv.size(); ++v) reach_ok = reach_ok && (g.reachable(0, v) == (lv[v] >= 0));
         std::printf("reach_matches_bfs %d\n", (int)reach_ok);
+        // incremental BFS / SSSP from vertex 0 (gir_test.cpp:1043-1083): cut 0's first out-edge,
+        // add one, update, and compare with from-scratch results
+        g.trackIncremental(0, false);
+        g.trackIncremental(0, true);
+        const auto out0 = g.getDirectedOutNeighbors(0);
+        if (!out0.empty()) g.deleteEdge(0, out0[0]);
+        g.insertEdge(g.vertexCount() - 1, 1);
+        g.updateIncremental(false);
+        g.updateIncremental(true);
+        const auto lv2 = g.bfs(0);
+        const auto d2 = g.sssp(0);
+        bool inc_ok = true;
+        for (int v = 0; v < (int)lv2.size(); ++v)
+            inc_ok = inc_ok && g.incDist(false, v) == (lv2[v] < 0 ? UINT64_MAX : (uint64_t)lv2[v]) &&
+                     g.incDist(true, v) == d2[v];
+        std::printf("inc_matches_scratch %d\n", (int)inc_ok);
         try {
             GIR bad("/nonexistent/dir/", "/nonexistent/dir/");
             std::printf("error_missing 0\n");

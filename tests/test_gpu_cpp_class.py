@@ -38,4 +38,5 @@ def test_cpp_caller_on_example_graph(golden, tmp_path):
     assert kv["bfs_0_9"][2] == str(golden["example/s3/sssp"][0][1])
     assert kv["has"] == ["1", "0", "1"]
     assert kv["reach_matches_bfs"] == ["1"]
+    assert kv["inc_matches_scratch"] == ["1"]
     assert kv["error_missing"] == ["1"]

@@ -119,3 +119,36 @@ def test_oracle_matches_reference_on_rmat(orc, pkg):
     np.testing.assert_array_equal(L2.wcc, r.wcc())
     np.testing.assert_array_equal(L2.blocks, r.blocks())
     r.close()
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref",
+                                                    "libgirref.so")), reason="reference not compiled here")
+def test_reference_incremental_matches_oracle(orc, pkg):
+    """Pins the incremental checker: the reference's own updateIncremental (gir_query.cpp:894-996)
+    equals the oracle's from-scratch BFS / SSSP after every batch of its IncTest pattern
+    (gir_test.cpp:1043-1083: mostly deletions of existing edges)."""
+    g = pkg.graphs.rmat(12, seed=7, weights=None)
+    fb, fa = orc.normalize(g.V, g.fw_beg, g.fw_adj)
+    r = orc.RefGIR(g.V, fb.astype(np.int32), fa, *orc.transpose(g.V, fb, fa))
+    r.build(7)
+    rng = np.random.default_rng(3)
+    src = int(np.argmax(np.diff(fb)))
+    r.inc_track(src, False)
+    r.inc_track(src, True)
+    none = np.uint64(2**64 - 1)
+    for _ in range(20):
+        beg, adj = r.out_csr()
+        a = rng.integers(0, g.V, 300)
+        a = a[beg[a + 1] > beg[a]]
+        b = adj[beg[a] + rng.integers(0, 1 << 30, len(a)) % (beg[a + 1] - beg[a])]
+        u = np.concatenate([a, rng.integers(0, g.V, 100)]).astype(np.int32)
+        v = np.concatenate([b, rng.integers(0, g.V, 100)]).astype(np.int32)
+        ins = np.concatenate([np.zeros(len(a)), np.ones(100)]).astype(np.uint8)
+        r.apply_batch(u, v, ins)
+        r.inc_update(False)
+        r.inc_update(True)
+        beg, adj = r.out_csr()
+        lv = orc.bfs(g.V, beg, adj, [src])
+        np.testing.assert_array_equal(r.inc_dist(False), np.where(lv < 0, none, lv.astype(np.uint64)))
+        np.testing.assert_array_equal(r.inc_dist(True), orc.sssp(g.V, beg, adj, [src]))
+    r.close()

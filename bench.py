@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-schedule", action="store_true", help="skip the learned-vs-fixed schedule comparison")
     p.add_argument("--no-batched", action="store_true", help="skip the batched queries + uneven batches section")
     p.add_argument("--no-incremental", action="store_true", help="skip the incremental BFS / SSSP section")
+    p.add_argument("--no-single", action="store_true", help="skip the single-edge update latency section")
     p.add_argument("--stream", type=int, default=0, metavar="ROUNDS",
                    help="instead of the bench: the 41.6M-vertex / 1.47B-edge R-MAT (seed 5, weights U[1,1023]), "
                         "WCC + SCC build, then ROUNDS x (1M-edge batch 60/40 + 32 BFS + 32 SSSP), checked by "
@@ -258,14 +259,90 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def incremental_section(pkg, d, stream, dev, src, with_ref):
+def reference_instance(pkg, d):
+    """The reference GIR (compiled from its sources) holding the device graph's current edges,
+    and the host seconds its construction took; None when the reference is not compiled here.
+    The device's create is timed on the same int32 arrays (sorted rows) beside it."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_available():
+        return None, {}
+    cb, ca = d.csr(0)
+    bb, ba = d.csr(1)
+    arrs = (cb.astype(np.int32), ca, bb.astype(np.int32), ba)
+    t = time.perf_counter()
+    ref = oracle.RefGIR(d.V, *arrs)
+    t_ref = time.perf_counter() - t
+    t = time.perf_counter()
+    d2 = pkg.DeviceGraph.create(*arrs, d.V)
+    t_dev = time.perf_counter() - t
+    d2.close()
+    return ref, {"device_s": t_dev, "reference_s": t_ref,
+                 "input": f"int32 four-array CSR of the current graph (V={d.V}, E={len(ca)}), host memory"}
+
+
+def single_edge_section(pkg, d, ref, n_ops=100):
+    """Single-edge updates (insertEdge / deleteEdge, gir.cpp:3043-3134) on the current graph with
+    every layer kept exact: n_ops ops alternating between deleting an existing edge and inserting
+    a random pair, one call each, host wall clock per call (the call returns after the device is
+    done). With ref the reference (its three layers built on the host cores first) takes the same
+    ops through updateEdgeDirected, and afterwards both WCC and SCC partitions must agree."""
+    import numpy as np
+    rng = np.random.default_rng(321)
+    V = d.V
+    cb, ca = d.csr(0)
+    ops = []
+    for i in range(n_ops):
+        if i % 2 == 0:
+            a = int(rng.integers(V))
+            while cb[a + 1] == cb[a]:
+                a = int(rng.integers(V))
+            ops.append((a, int(ca[cb[a] + rng.integers(cb[a + 1] - cb[a])]), 0))
+        else:
+            a, b = int(rng.integers(V)), int(rng.integers(V))
+            ops.append((a, b if b != a else (a + 1) % V, 1))
+    res = {"ops": n_ops}
+    if ref is not None:
+        for mask, name in ((1, "wcc"), (2, "scc_dag"), (4, "bct")):
+            t = time.perf_counter()
+            ref.build(mask)
+            res[f"ref_build_{name}_s"] = time.perf_counter() - t
+        res["ref_threads"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    st0 = d.single_stats()
+    dev_ms, plans = [], {"wcc": {}, "scc": {}, "bct": {}}
+    for a, b, i in ops:
+        t = time.perf_counter()
+        d.apply_batch(np.array([a], np.int32), np.array([b], np.int32), np.array([i], np.uint8))
+        dev_ms.append((time.perf_counter() - t) * 1e3)
+        for k, x in d.batch_plan().items():
+            plans[k][x] = plans[k].get(x, 0) + 1
+    st1 = d.single_stats()
+    res.update(device_median_ms=float(np.median(dev_ms)), device_mean_ms=float(np.mean(dev_ms)),
+               device_p90_ms=float(np.percentile(dev_ms, 90)), layer_decisions=plans,
+               checked=st1["checked"] - st0["checked"], rebuilds_avoided=st1["kept"] - st0["kept"])
+    if ref is not None:
+        ref_ms = []
+        for a, b, i in ops:
+            t = time.perf_counter()
+            ref.update_edge(a, b, bool(i))
+            ref_ms.append((time.perf_counter() - t) * 1e3)
+        res.update(ref_median_ms=float(np.median(ref_ms)), ref_mean_ms=float(np.mean(ref_ms)),
+                   ref_p90_ms=float(np.percentile(ref_ms, 90)))
+        res["scc_identical_to_reference"] = bool(np.array_equal(d.labels(pkg.native.LABEL_SCC), ref.scc()))
+        res["wcc_identical_to_reference"] = bool(np.array_equal(d.labels(pkg.native.LABEL_WCC), ref.wcc()))
+    return res
+
+
+def incremental_section(pkg, d, stream, dev, src, ref):
     """Incremental single-source BFS / SSSP (GIR::trackIncremental / updateIncremental) on the
     current graph: batches of 1K / 10K / 100K ops (two thirds deletions of existing edges, one third
     random insertions), each applied (untimed here) and followed by the update of both tracked
     results, timed against a from-scratch query of the same source; after every update both results
     must equal the from-scratch ones. With with_ref the reference (compiled from its sources) tracks
     the same source and takes the same batches (ingestBatch); its updateIncremental is timed on the
-    host cores beside the device's and its results must equal the device's."""
+    host cores beside the device's and its results must equal the device's (ref: the instance
+    from reference_instance, or None)."""
     import numpy as np
     import torch
     V = d.V
@@ -280,18 +357,12 @@ def incremental_section(pkg, d, stream, dev, src, with_ref):
            "track_ms": {"sssp": ev_time(stream, lambda: d.inc_track(src, True)),
                         "bfs": ev_time(stream, lambda: d.inc_track(src, False))}, "batches": {}}
     cb, ca = d.csr(0)
-    ref = None
-    if with_ref:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle
-        if oracle.ref_available():
-            bb, ba = d.csr(1)
-            ref = oracle.RefGIR(V, cb.astype(np.int32), ca, bb.astype(np.int32), ba)
-            t = time.perf_counter()
-            ref.inc_track(src, True)
-            ref.inc_track(src, False)
-            res["ref_track_s"] = time.perf_counter() - t
-            res["ref_threads"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    if ref is not None:
+        t = time.perf_counter()
+        ref.inc_track(src, True)
+        ref.inc_track(src, False)
+        res["ref_track_s"] = time.perf_counter() - t
+        res["ref_threads"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
     none = np.iinfo(np.uint64).max
     for k in (1_000, 10_000, 100_000):
         a = rng.integers(0, V, 2 * k // 3)
@@ -329,8 +400,6 @@ def incremental_section(pkg, d, stream, dev, src, with_ref):
             assert dw[src] == 0 and db[src] == 0 and (dw != none).sum() == (db != none).sum()
         res["batches"][str(k)] = row
         cb, ca = d.csr(0)
-    if ref is not None:
-        ref.close()
     return res
 
 
@@ -632,10 +701,19 @@ def run_ours(args):
         bc_out = torch.empty(V, dtype=torch.float64, device=dev)
         t_bc = ev_time(stream, lambda: d.bc(sb_d, out=bc_out))
         extra["bc_64_sources_ms"] = t_bc
+        # the reference on the host cores, holding the same graph (create timed beside the device's)
+        ref = None
+        if rank == 0 and world == 1 and not args.no_cpu:
+            ref, extra["create_from_csr"] = reference_instance(pkg, d)
+        # single-edge update latency (every layer kept exact), beside the reference's; first, since
+        # the reference's single-edge entry points sync the batches ingestBatch leaves pending
+        if not args.no_single:
+            extra["single_edge_updates"] = single_edge_section(pkg, d, ref)
         # incremental BFS / SSSP of one source under 1K / 10K / 100K-op batches
         if not args.no_incremental:
-            extra["incremental"] = incremental_section(pkg, d, stream, dev, int(sb_d[0].item()),
-                                                       rank == 0 and world == 1 and not args.no_cpu)
+            extra["incremental"] = incremental_section(pkg, d, stream, dev, int(sb_d[0].item()), ref)
+        if ref is not None:
+            ref.close()
         extra["reachable"] = {"pairs": n_r, "ms": t_r, "pairs_per_s": n_r / (t_r * 1e-3),
                               "true_fraction": float(rout.float().mean().item())}
         if rep is not None:

@@ -440,6 +440,9 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     }
     unsigned long long hc[2] = {0, 0};
     cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, g->stream);
+    uint64_t one_key = 0;  // the change of a batch with exactly one (the single-edge latency path)
+    if (n_ins + n_del == 1)
+        cudaMemcpyAsync(&one_key, n_ins ? ins_k : del_k, sizeof(uint64_t), cudaMemcpyDeviceToHost, g->stream);
     if ((rc = cuda_check(g, cudaStreamSynchronize(g->stream), "batch counters"))) { cleanup(); return rc; }
     cleanup();
     g->b_invalid = (int64_t)hc[0];
@@ -527,6 +530,21 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     plan.n_pairs_in = nsi;
     plan.scc = (fl[F_SCC_SPLIT] || fl[F_SCC_CYCLE]) ? REBUILD : (fl[F_DAG] ? PATCH : KEEP);
     plan.bct = fl[F_BCT] ? REBUILD : KEEP;
+    if (n_ins + n_del == 1) {
+        // one change: exact searches settle what the flags leave open (single.cu)
+        SingleChecks want;
+        want.wcc = g->wcc_built && nsd > 0;
+        want.split = g->scc_built && fl[F_SCC_SPLIT];
+        want.cycle = g->scc_built && fl[F_SCC_CYCLE];
+        want.twopath = g->bct_built && fl[F_BCT] && n_del == 1 && nsd > 0;
+        int32_t res[4];
+        GIR_TRY(single_op_checks(g, (int32_t)(one_key >> 32), (int32_t)(uint32_t)one_key, want, res));
+        if (want.wcc || want.split || want.cycle || want.twopath) ++g->single_checked;
+        if (want.wcc && res[0] == 1) { plan.wcc = KEEP; ++g->single_kept; }
+        if (want.split && res[1] == 1) { plan.scc = fl[F_DAG] ? PATCH : KEEP; ++g->single_kept; }
+        if (want.cycle && res[2] == 2) { plan.scc = PATCH; ++g->single_kept; }
+        if (want.twopath && res[3] == 1 && plan.scc != REBUILD) { plan.bct = KEEP; ++g->single_kept; }
+    }
     g->b_plan[0] = plan.wcc;
     g->b_plan[1] = plan.scc;
     g->b_plan[2] = plan.scc == REBUILD ? REBUILD : plan.bct;
@@ -669,7 +687,7 @@ int gir_dev_destroy(gir_dev_t* g) {
         store_free(g, g->ws[0]); store_free(g, g->ws[1]);
         for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->dag_rows, &g->reach_hub, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
                           &g->cub_tmp, &g->stage_in, &g->stage_out, &g->sched_w, &g->sched_io, &g->lane_dist, &g->inc_st[0], &g->inc_st[1],
-                          &g->inc_pend[0], &g->inc_pend[1]})
+                          &g->inc_pend[0], &g->inc_pend[1], &g->single_ws})
             release(g, *b);
         for (auto& b : g->scratch) release(g, b);
         for (auto& b : g->work) release(g, b);
@@ -869,6 +887,13 @@ int gir_dev_bc(gir_dev_t* g, const int32_t* srcs, int64_t n_src, double* score_o
     release(g, ss);
     release_scratch(g, kKeepScratchBelow);
     return rc;
+}
+
+int gir_dev_single_stats(gir_dev_t* g, int64_t* checked, int64_t* kept) {
+    if (!g) return GIR_ERR_INVALID;
+    if (checked) *checked = g->single_checked;
+    if (kept) *kept = g->single_kept;
+    return GIR_OK;
 }
 
 int gir_dev_inc_track(gir_dev_t* g, int32_t source, int weighted) {

@@ -112,6 +112,11 @@ struct gir_dev {
     gir::DevBuf inc_st[2], inc_pend[2];
     int64_t inc_npend[2] = {0, 0};
 
+    // Working arrays of the single-edge checks (single.cu): generation-stamped, zeroed once.
+    gir::DevBuf single_ws;
+    int32_t single_gen = 1;
+    int64_t single_checked = 0, single_kept = 0;  // ops that ran the checks / rebuilds they avoided
+
     // Weight-sorted copies of the forward CSR for SSSP ([0] hash weights, [1] stored weights).
     gir::DevCSR ws[2];
     bool ws_valid[2] = {false, false};
@@ -269,6 +274,14 @@ int bc_run(gir_dev* g, const int32_t* srcs_d, int64_t n_src, double* score_d);
 // Reachability of every pair (u[i], v[i]) into out[i] (device arrays; the SCC layer is built).
 int reach_run(gir_dev* g, const int32_t* u_d, const int32_t* v_d, int64_t n, uint8_t* out_d);
 int bct_build(gir_dev* g);
+// Exact checks for a batch with one effective edge change u -> v (single.cu); out[i] per check:
+// 0 not run, 1 found, 2 not found, 3 over budget (unknown). wcc: u, v connected in sym. split:
+// u reaches v inside their SCC. cycle: v reaches u within the rank window. twopath: two
+// internally vertex-disjoint u-v paths in their SCC's undirected subgraph.
+struct SingleChecks {
+    bool wcc = false, split = false, cycle = false, twopath = false;
+};
+int single_op_checks(gir_dev* g, int32_t u, int32_t v, const SingleChecks& want, int32_t out[4]);
 // Incremental BFS / SSSP (incr.cu): track one source, log a batch's changed edges (device keys),
 // correct the tracked result for the logged changes, and write its distances (device, V entries).
 int inc_track(gir_dev* g, int32_t source, int weighted);

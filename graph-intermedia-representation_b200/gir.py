@@ -226,6 +226,12 @@ class DeviceGraph:
         self._ck(dev_lib().gir_dev_inc_dist(self._h, 1 if weighted else 0, ptr(res)), "inc_dist")
         return res
 
+    def single_stats(self):
+        """One-op batches that ran the exact single-edge checks, and the layer rebuilds they avoided."""
+        c, k = ctypes.c_int64(), ctypes.c_int64()
+        self._ck(dev_lib().gir_dev_single_stats(self._h, ctypes.byref(c), ctypes.byref(k)), "single_stats")
+        return {"checked": c.value, "kept": k.value}
+
     def batch_plan(self):
         """Per layer, what the last batch did: 'kept', 'patched' or 'rebuilt'."""
         out = np.zeros(3, np.int32)

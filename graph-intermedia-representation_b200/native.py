@@ -35,7 +35,7 @@ DEV_SYMBOLS = (
     "gir_dev_sched_get_weights", "gir_dev_sched_param_count", "gir_dev_sched_train", "gir_dev_sched_forward",
     "gir_dev_sched_grad", "gir_dev_bfs_noalloc", "gir_dev_sched_trace", "gir_dev_sched_delta_choices",
     "gir_dev_batch_times", "gir_dev_batch_plan", "gir_dev_autotune", "gir_dev_reachable", "gir_dev_bc",
-    "gir_dev_inc_track", "gir_dev_inc_update", "gir_dev_inc_dist",
+    "gir_dev_inc_track", "gir_dev_inc_update", "gir_dev_inc_dist", "gir_dev_single_stats",
 )
 GEN_SYMBOLS = (
     "gir_gen_last_error", "gir_gen_free", "gir_gen_hash3", "gir_gen_rmat", "gir_gen_lattice", "gir_gen_csr",
@@ -114,6 +114,7 @@ def dev_lib():
             "gir_dev_inc_track": [_P, _I32, ctypes.c_int],
             "gir_dev_inc_update": [_P, ctypes.c_int],
             "gir_dev_inc_dist": [_P, ctypes.c_int, _P],
+            "gir_dev_single_stats": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
         }
         for name, args in sig.items():
             f = getattr(lib, name)

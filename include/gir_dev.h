@@ -199,6 +199,14 @@ int gir_dev_inc_dist(gir_dev_t* g, int weighted, uint64_t* dist_out);
 /* Weight rule for edges inserted into a graph with stored weights (see apply_batch). */
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi);
 
+/* The single-edge latency path (insertEdge / deleteEdge, gir.cpp:3043-3134, as one-op batches):
+ * a batch with exactly one effective change settles what its layer flags leave open with exact
+ * device searches (u, v still connected; u still reaching v inside its SCC; no cycle closed by an
+ * insert against the rank order; two vertex-disjoint u-v paths left inside the SCC, so its blocks
+ * stand) instead of rebuilding the layer. Counters since create: *checked = such batches that ran
+ * a search, *kept = layer rebuilds the searches avoided. Either pointer may be NULL. */
+int gir_dev_single_stats(gir_dev_t* g, int64_t* checked, int64_t* kept);
+
 /* Counters of the last apply_batch: inserted / deleted edges that changed the graph, no-op and
  * invalid operations. Any pointer may be NULL. */
 int gir_dev_batch_stats(gir_dev_t* g, int64_t* n_ins, int64_t* n_del, int64_t* n_noop, int64_t* n_invalid);

@@ -226,6 +226,58 @@ def test_batch_repair_plans_match_oracle(pkg, orc, s16):
     assert "patched" in seen["wcc"] or "kept" in seen["wcc"], seen
 
 
+def test_single_edge_checks_match_oracle(pkg, orc):
+    """One-op batches (the single-edge latency path, insertEdge / deleteEdge) whose layer decisions
+    come from the exact device searches, checked against the oracle after every op: deletions of
+    existing edges inside SCCs and anywhere, inserts against the rank order (closing a cycle or
+    not) and random inserts, on a dense R-MAT (one big SCC and block) and a sparse one (bridges,
+    articulation points, small SCCs). The searches must keep layers many times, and layers must
+    still be patched and rebuilt where the searches say so."""
+    seen = {"wcc": set(), "scc": set(), "bct": set()}
+    checked = kept = 0
+    for ef, n_ops in ((16, 120), (2, 200)):
+        g = pkg.graphs.rmat(11, n_draws=ef << 11, seed=40 + ef, weights=None)
+        V = g.V
+        fb, fa = orc.normalize(V, g.fw_beg, g.fw_adj)
+        d = pkg.DeviceGraph.from_graph(g, weights=False)
+        d.build(pkg.native.LAYER_ALL)
+        rng = np.random.default_rng(ef)
+        for i in range(n_ops):
+            scc = d.labels(pkg.native.LABEL_SCC)
+            rank = d.labels(pkg.native.LABEL_SCC_RANK)
+            kind = i % 4
+            if kind in (0, 1):  # delete an existing edge (kind 0: one inside an SCC if any)
+                rows = np.repeat(np.arange(V), np.diff(fb))
+                cand = np.nonzero(scc[rows] == scc[fa])[0] if kind == 0 else np.arange(len(fa))
+                if len(cand) == 0:
+                    cand = np.arange(len(fa))
+                j = int(rng.choice(cand))
+                u, v, ins = int(rows[j]), int(fa[j]), 0
+            elif kind == 2:  # insert against the rank order
+                a, c = rng.integers(0, V, 256), rng.integers(0, V, 256)
+                back = np.nonzero((scc[a] != scc[c]) & (rank[a] > rank[c]))[0]
+                if len(back) == 0:
+                    continue
+                u, v, ins = int(a[back[0]]), int(c[back[0]]), 1
+            else:
+                u, v, ins = int(rng.integers(V)), int(rng.integers(V)), 1
+                if u == v:
+                    continue
+            d.apply_batch(np.array([u], np.int32), np.array([v], np.int32), np.array([ins], np.uint8))
+            for k, x in d.batch_plan().items():
+                seen[k].add(x)
+            fb, fa, _, _ = orc.apply_batch(V, fb, fa, [u], [v], [ins])
+            _oracle_match(pkg, orc, d, V, fb, fa, f"op {i} ({u} -> {v}, insert {ins}), edge factor {ef}")
+        st = d.single_stats()
+        checked += st["checked"]
+        kept += st["kept"]
+        d.close()
+    assert checked > 100 and kept > 50, (checked, kept)
+    assert {"kept", "rebuilt"} <= seen["wcc"], seen
+    assert {"kept", "patched", "rebuilt"} <= seen["scc"], seen
+    assert {"kept", "rebuilt"} <= seen["bct"], seen
+
+
 def test_reachable_matches_reference(pkg, orc, s16):
     """Batched reachability against the reference's own GIR::reachable (compiled from its
     sources) and the oracle's BFS, before and after a batch: random pairs, same-SCC pairs,

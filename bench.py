@@ -310,16 +310,25 @@ def single_edge_section(pkg, d, ref, n_ops=100):
             res[f"ref_build_{name}_s"] = time.perf_counter() - t
         res["ref_threads"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
     st0 = d.single_stats()
-    dev_ms, plans = [], {"wcc": {}, "scc": {}, "bct": {}}
+    dev_ms, plans, phases = [], {"wcc": {}, "scc": {}, "bct": {}}, {0: [], 1: []}
     for a, b, i in ops:
         t = time.perf_counter()
         d.apply_batch(np.array([a], np.int32), np.array([b], np.int32), np.array([i], np.uint8))
         dev_ms.append((time.perf_counter() - t) * 1e3)
+        ph = d.batch_times()
+        ph["checks"] = dev_ms[-1] - sum(ph.values())  # (the searches run between the phases)
+        phases[i].append(ph)
         for k, x in d.batch_plan().items():
             plans[k][x] = plans[k].get(x, 0) + 1
     st1 = d.single_stats()
+    by_kind = {}
+    for i, name in ((0, "delete"), (1, "insert")):
+        ms = [sum(p.values()) for p in phases[i]]
+        by_kind[name] = {"median_ms": float(np.median(ms)),
+                         "phase_median_ms": {k: round(float(np.median([p[k] for p in phases[i]])), 3)
+                                             for k in phases[i][0]}}
     res.update(device_median_ms=float(np.median(dev_ms)), device_mean_ms=float(np.mean(dev_ms)),
-               device_p90_ms=float(np.percentile(dev_ms, 90)), layer_decisions=plans,
+               device_p90_ms=float(np.percentile(dev_ms, 90)), by_kind=by_kind, layer_decisions=plans,
                checked=st1["checked"] - st0["checked"], rebuilds_avoided=st1["kept"] - st0["kept"])
     if ref is not None:
         ref_ms = []

@@ -364,6 +364,9 @@ struct RepairPlan {
     int wcc = REBUILD, scc = REBUILD, bct = REBUILD;
     const uint64_t* pairs_in = nullptr;  // newly present undirected pairs (both orientations)
     int64_t n_pairs_in = 0;
+    bool one_edge = false;  // SCC PATCH for one change that respects the ranks: one DAG key
+    int32_t u = 0, v = 0;
+    bool insert = false;
 };
 
 // Brings every built layer up to date, timing each (phases 1..3 of gir_dev_batch_times).
@@ -378,7 +381,13 @@ int rebuild_layers(gir_dev* g, const RepairPlan& plan) {
     t = now_ms();
     if (g->scc_built) {
         if (plan.scc == REBUILD) GIR_TRY(scc_build(g));
-        else if (plan.scc == PATCH) GIR_TRY(scc_build_dag(g));
+        else if (plan.scc == PATCH && plan.one_edge) {
+            bool patched = false;
+            GIR_TRY(scc_dag_patch_one(g, plan.u, plan.v, plan.insert, &patched));
+            if (patched) ++g->single_kept;
+        } else if (plan.scc == PATCH) {
+            GIR_TRY(scc_build_dag(g));
+        }
     }
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     g->b_ms[2] = now_ms() - t;
@@ -541,9 +550,20 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
         GIR_TRY(single_op_checks(g, (int32_t)(one_key >> 32), (int32_t)(uint32_t)one_key, want, res));
         if (want.wcc || want.split || want.cycle || want.twopath) ++g->single_checked;
         if (want.wcc && res[0] == 1) { plan.wcc = KEEP; ++g->single_kept; }
+        if (want.wcc && res[0] == 4) {  // the component split, labels already updated in place
+            plan.wcc = KEEP;
+            ++g->n_wcc;
+            ++g->single_kept;
+        }
         if (want.split && res[1] == 1) { plan.scc = fl[F_DAG] ? PATCH : KEEP; ++g->single_kept; }
         if (want.cycle && res[2] == 2) { plan.scc = PATCH; ++g->single_kept; }
         if (want.twopath && res[3] == 1 && plan.scc != REBUILD) { plan.bct = KEEP; ++g->single_kept; }
+        if (plan.scc == PATCH && !fl[F_SCC_CYCLE]) {  // a cross-SCC change along the rank order
+            plan.one_edge = true;
+            plan.u = (int32_t)(one_key >> 32);
+            plan.v = (int32_t)(uint32_t)one_key;
+            plan.insert = n_ins == 1;
+        }
     }
     g->b_plan[0] = plan.wcc;
     g->b_plan[1] = plan.scc;

@@ -269,13 +269,18 @@ int wcc_union_pairs(gir_dev* g, const uint64_t* keys, int64_t n);
 int scc_build(gir_dev* g);
 // Condensation DAG and ranks from the current SCC labels (the labels are kept).
 int scc_build_dag(gir_dev* g);
+// The DAG after one edge u -> v between two SCCs whose ranks respect it was inserted or deleted
+// (labels unchanged): one key added or removed where that settles it (*patched), else
+// scc_build_dag.
+int scc_dag_patch_one(gir_dev* g, int32_t u, int32_t v, bool insert, bool* patched);
 // Betweenness of every vertex over the sources (device arrays; score has V entries).
 int bc_run(gir_dev* g, const int32_t* srcs_d, int64_t n_src, double* score_d);
 // Reachability of every pair (u[i], v[i]) into out[i] (device arrays; the SCC layer is built).
 int reach_run(gir_dev* g, const int32_t* u_d, const int32_t* v_d, int64_t n, uint8_t* out_d);
 int bct_build(gir_dev* g);
 // Exact checks for a batch with one effective edge change u -> v (single.cu); out[i] per check:
-// 0 not run, 1 found, 2 not found, 3 over budget (unknown). wcc: u, v connected in sym. split:
+// 0 not run, 1 found, 2 not found, 3 over budget (unknown), 4 (wcc only) not connected, and the
+// component's labels were split in place. wcc: u, v connected in sym. split:
 // u reaches v inside their SCC. cycle: v reaches u within the rank window. twopath: two
 // internally vertex-disjoint u-v paths in their SCC's undirected subgraph.
 struct SingleChecks {

@@ -433,6 +433,103 @@ int scc_build(gir_dev* g) {
     return scc_build_dag(g);
 }
 
+// One edge u -> v between two SCCs (u's SCC before v's in rank order), inserted or just deleted:
+// out[0] = position of its condensation key in the sorted keys (lower bound), out[1] = the key is
+// there; out[2] bit 0 = another edge joins the two SCCs from u's forward row or v's backward
+// row, bit 1 = u has an out-neighbour in its own SCC, bit 2 = v has an in-neighbour in its own
+// SCC (a vertex of a non-trivial SCC always has both, so without them both SCCs are singletons
+// and the two rows are every edge between them).
+__global__ void k_dag_probe(const uint64_t* dag, int64_t n, uint64_t key, CSRView fw, CSRView bw,
+                            const int32_t* label, int32_t u, int32_t v, unsigned long long* out) {
+    const int32_t cu = label[u], cv = label[v];
+    unsigned long long bits = 0;
+    for (int64_t k = fw.beg[u] + threadIdx.x; k < fw.beg[u] + fw.deg[u]; k += blockDim.x) {
+        const int32_t y = label[fw.adj[k]];
+        if (y == cv) bits |= 1;
+        if (y == cu) bits |= 2;
+    }
+    for (int64_t k = bw.beg[v] + threadIdx.x; k < bw.beg[v] + bw.deg[v]; k += blockDim.x) {
+        const int32_t x = label[bw.adj[k]];
+        if (x == cu) bits |= 1;
+        if (x == cv) bits |= 4;
+    }
+    if (bits) atomicOr(&out[2], bits);
+    if (threadIdx.x == 0) {
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const int64_t m = (lo + hi) >> 1;
+            if (dag[m] < key) lo = m + 1; else hi = m;
+        }
+        out[0] = (unsigned long long)lo;
+        out[1] = lo < n && dag[lo] == key;
+    }
+}
+
+__global__ void k_dag_put(uint64_t* dag, int64_t p, uint64_t key) { dag[p] = key; }
+
+int scc_dag_patch_one(gir_dev* g, int32_t u, int32_t v, bool insert, bool* patched) {
+    *patched = false;
+    const int32_t* label = static_cast<const int32_t*>(g->scc.p);
+    const int64_t n = g->n_dag;
+    if (n < 0 || !g->dag.p || u < 0 || v < 0 || u >= g->V || v >= g->V) return scc_build_dag(g);
+    unsigned long long* cnt = nullptr;
+    GIR_TRY(ensure_n(g, g->scratch[6], 2 * C_N, &cnt));
+    void* hp = nullptr;
+    GIR_TRY(pinned(g, 256, &hp));
+    unsigned long long* hc = static_cast<unsigned long long*>(hp);
+    int32_t lab[2];
+    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 3, g->stream));
+    GIR_CUDA(g, cudaMemcpyAsync(&lab[0], label + u, sizeof(int32_t), cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaMemcpyAsync(&lab[1], label + v, sizeof(int32_t), cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    const uint64_t key = ((uint64_t)(uint32_t)lab[0] << 32) | (uint32_t)lab[1];
+    k_dag_probe<<<1, kBlock, 0, g->stream>>>(static_cast<const uint64_t*>(g->dag.p), n, key, view(g->fw), view(g->bw),
+                                             label, u, v, cnt);
+    GIR_LAUNCH(g, "k_dag_probe");
+    GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * 3, cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    const int64_t p = (int64_t)hc[0];
+    const bool present = hc[1] != 0;
+    const unsigned long long bits = hc[2];
+    uint64_t* dag = static_cast<uint64_t*>(g->dag.p);
+    if (insert) {
+        if (present) {
+            *patched = true;  // the SCCs were joined already
+            return GIR_OK;
+        }
+        if (g->dag.bytes < sizeof(uint64_t) * (size_t)(n + 2)) return scc_build_dag(g);
+        uint64_t* tmp = nullptr;
+        GIR_TRY(ensure_n(g, g->scratch[8], n - p + 1, &tmp));
+        if (n > p) {
+            GIR_CUDA(g, cudaMemcpyAsync(tmp, dag + p, sizeof(uint64_t) * (n - p), cudaMemcpyDeviceToDevice, g->stream));
+            GIR_CUDA(g, cudaMemcpyAsync(dag + p + 1, tmp, sizeof(uint64_t) * (n - p), cudaMemcpyDeviceToDevice, g->stream));
+        }
+        k_dag_put<<<1, 1, 0, g->stream>>>(dag, p, key);
+        GIR_LAUNCH(g, "k_dag_put");
+        g->n_dag = n + 1;
+    } else {
+        if (!present || (bits & 1)) {
+            *patched = true;  // another edge still joins the two SCCs (or none was recorded)
+            return GIR_OK;
+        }
+        if (bits & 6) return scc_build_dag(g);  // a non-trivial SCC: its other members' rows count too
+        if (n - p - 1 > 0) {
+            uint64_t* tmp = nullptr;
+            GIR_TRY(ensure_n(g, g->scratch[8], n - p, &tmp));
+            GIR_CUDA(g, cudaMemcpyAsync(tmp, dag + p + 1, sizeof(uint64_t) * (n - p - 1), cudaMemcpyDeviceToDevice,
+                                        g->stream));
+            GIR_CUDA(g, cudaMemcpyAsync(dag + p, tmp, sizeof(uint64_t) * (n - p - 1), cudaMemcpyDeviceToDevice,
+                                        g->stream));
+        }
+        g->n_dag = n - 1;
+    }
+    // the ranks stay a topological order (the edge respects them); reachability changed
+    g->dag_rows_valid = false;
+    g->reach_hub_valid = false;
+    *patched = true;
+    return GIR_OK;
+}
+
 int scc_build_dag(gir_dev* g) {
     const int64_t V = g->V;
     int32_t* label = static_cast<int32_t*>(g->scc.p);

@@ -13,7 +13,8 @@
 //    the block that held {u, v} stays biconnected exactly then, so every block is unchanged.
 //    One path P1 comes from a bidirectional search; the second from one augmenting search in the
 //    residual graph of P1 with every vertex split into an entered and a left state.
-// All searches run in one CTA of one launch (no host round trip per level) with visited marks
+// A WCC split found this way is applied in place (the search that ran out holds the whole new
+// component). All searches run in one CTA of one launch (no host round trip per level) with visited marks
 // stamped by generation, so nothing is cleared between calls, and with budgets on visited
 // vertices and scanned edges: a search that exceeds them reports "unknown" and the layer is
 // rebuilt as before.
@@ -30,7 +31,8 @@ constexpr unsigned long long kEdgeBudget = 1ull << 22;
 constexpr int kVisitBudget = 1 << 20;
 constexpr unsigned kFull = 0xffffffffu;
 
-enum { R_NOT_RUN = 0, R_FOUND = 1, R_NONE = 2, R_UNKNOWN = 3 };
+// R_SPLIT: not connected, and the WCC labels were split in place
+enum { R_NOT_RUN = 0, R_FOUND = 1, R_NONE = 2, R_UNKNOWN = 3, R_SPLIT = 4 };
 
 // Working arrays (int32 each), sections of one buffer of kWords * V entries.
 struct Work {
@@ -61,8 +63,10 @@ struct Shared {
     int found;                 // meeting vertex (or target state) + 1
     int nbig;
     unsigned long long edges;  // scanned edges (budget)
+    unsigned long long fe, be, ne;  // row entries of the forward / backward frontier; of the next one
     int lo_f, hi_f, lo_b, hi_b;
     int result;
+    int mn;
     int32_t big[kBig];
 };
 
@@ -115,8 +119,10 @@ __device__ __forceinline__ bool claim(int32_t* stamp, int32_t y, int32_t gen) {
 __device__ __forceinline__ int32_t same_vertex(int32_t x) { return x; }
 
 // Bidirectional search from s (over fwd) and t (over bwd), both sides limited by the filter,
-// expanding the smaller frontier each level. R_FOUND with S.found = meeting vertex + 1; R_NONE
-// when one side ran out first (t is not reachable from s); R_UNKNOWN over budget.
+// expanding each level the side whose frontier has fewer row entries (the work of the level, so
+// a side that has reached a hub waits while the other side catches up). R_FOUND with S.found =
+// meeting vertex + 1; R_NONE when one side ran out first (t is not reachable from s); R_UNKNOWN
+// over budget.
 __device__ int bidir(const CSRView& fwd, const CSRView& bwd, const Filter& F, int32_t s, int32_t t, int32_t gen,
                      const Work& W, Shared& S) {
     if (threadIdx.x == 0) {
@@ -129,6 +135,8 @@ __device__ int bidir(const CSRView& fwd, const CSRView& bwd, const Filter& F, in
         S.found = s == t ? s + 1 : 0;
         S.stop = S.found != 0;
         S.edges = 0;
+        S.fe = (unsigned long long)fwd.deg[s];
+        S.be = (unsigned long long)bwd.deg[t];
         S.lo_f = S.lo_b = 0;
         S.hi_f = S.hi_b = 1;
         S.result = S.found ? R_FOUND : R_NOT_RUN;
@@ -144,15 +152,19 @@ __device__ int bidir(const CSRView& fwd, const CSRView& bwd, const Filter& F, in
             if (threadIdx.x == 0) S.result = R_UNKNOWN;
             break;
         }
-        const bool fside = (S.hi_f - S.lo_f) <= (S.hi_b - S.lo_b);
+        const bool fside = S.fe <= S.be;
         const int lo = fside ? S.lo_f : S.lo_b, hi = fside ? S.hi_f : S.hi_b;
         __syncthreads();  // (every thread has read the bounds before thread 0 moves them)
-        if (threadIdx.x == 0) S.tail = hi;
+        if (threadIdx.x == 0) {
+            S.tail = hi;
+            S.ne = 0;
+        }
         if (fside) {
             cta_expand(fwd, W.q_f, lo, hi, S, same_vertex, [&](int32_t x, int32_t y) {
                 if (!F.ok(y) || !claim(W.stamp_f, y, gen)) return;
                 W.par_f[y] = x;
                 W.q_f[atomicAdd(&S.tail, 1)] = y;
+                atomicAdd(&S.ne, (unsigned long long)fwd.deg[y]);
                 if (W.stamp_b[y] == gen) {
                     S.found = y + 1;
                     S.stop = 1;
@@ -163,6 +175,7 @@ __device__ int bidir(const CSRView& fwd, const CSRView& bwd, const Filter& F, in
                 if (!F.ok(y) || !claim(W.stamp_b, y, gen)) return;
                 W.par_b[y] = x;
                 W.q_b[atomicAdd(&S.tail, 1)] = y;
+                atomicAdd(&S.ne, (unsigned long long)bwd.deg[y]);
                 if (W.stamp_f[y] == gen) {
                     S.found = y + 1;
                     S.stop = 1;
@@ -170,7 +183,15 @@ __device__ int bidir(const CSRView& fwd, const CSRView& bwd, const Filter& F, in
             });
         }
         if (threadIdx.x == 0) {
-            if (fside) { S.lo_f = hi; S.hi_f = S.tail; } else { S.lo_b = hi; S.hi_b = S.tail; }
+            if (fside) {
+                S.lo_f = hi;
+                S.hi_f = S.tail;
+                S.fe = S.ne;
+            } else {
+                S.lo_b = hi;
+                S.hi_b = S.tail;
+                S.be = S.ne;
+            }
             if (S.stop) S.result = R_FOUND;
         }
         __syncthreads();
@@ -259,10 +280,43 @@ __device__ int second_path(const CSRView& sym, const Filter& F, int32_t u, int32
     return r;
 }
 
+// A removed undirected pair split its weakly connected component (label L) in two. The side of
+// the search that ran out first visited all of its part (set[0..n), stamped gen), so: that part
+// takes its smallest id as label, unless L itself lies in it, in which case the part keeps L and
+// the rest of the old component takes the rest's smallest id (one CTA pass over the labels).
+__device__ void wcc_split(int32_t* label, int64_t V, int32_t L, const int32_t* set, int n, const int32_t* stamp,
+                          int32_t gen, Shared& S) {
+    if (threadIdx.x == 0) S.mn = INT32_MAX;
+    __syncthreads();
+    int32_t m = INT32_MAX;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = set[i] < m ? set[i] : m;
+    atomicMin(&S.mn, m);
+    __syncthreads();
+    const int32_t ms = S.mn;
+    __syncthreads();
+    if (ms != L) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) label[set[i]] = ms;
+    } else {
+        if (threadIdx.x == 0) S.mn = INT32_MAX;
+        __syncthreads();
+        int32_t m2 = INT32_MAX;
+        for (int64_t x = threadIdx.x; x < V; x += blockDim.x)
+            if (label[x] == L && stamp[x] != gen) m2 = (int32_t)x < m2 ? (int32_t)x : m2;
+        atomicMin(&S.mn, m2);
+        __syncthreads();
+        const int32_t mr = S.mn;
+        if (mr != INT32_MAX)
+            for (int64_t x = threadIdx.x; x < V; x += blockDim.x)
+                if (label[x] == L && stamp[x] != gen) label[x] = mr;
+    }
+    __syncthreads();
+}
+
 struct CheckArgs {
     CSRView fw, bw, sym;
     const int32_t* scc;
     const int32_t* rank;
+    int32_t* wcc_label;  // split in place when the WCC check finds u, v disconnected
     int64_t V;
     int32_t u, v;
     int wcc, split, cycle, twopath;
@@ -276,25 +330,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_single_checks(CheckArgs a) {
     const int32_t u = a.u, v = a.v;
     const Filter none{nullptr, 0, nullptr, 0, 0};
     int r = R_NOT_RUN;
-    if (a.wcc) r = bidir(a.sym, a.sym, none, u, v, a.gen0, a.W, S);
-    if (threadIdx.x == 0) a.out[0] = r;
-    r = R_NOT_RUN;
-    if (a.split) {
-        const Filter f{a.scc, a.scc[u], nullptr, 0, 0};
-        r = bidir(a.fw, a.bw, f, u, v, a.gen0 + 1, a.W, S);
-    }
-    if (threadIdx.x == 0) a.out[1] = r;
-    r = R_NOT_RUN;
-    if (a.cycle) {
-        const Filter f{nullptr, 0, a.rank, a.rank[v], a.rank[u]};
-        r = bidir(a.fw, a.bw, f, v, u, a.gen0 + 2, a.W, S);
-    }
-    if (threadIdx.x == 0) a.out[2] = r;
-    r = R_NOT_RUN;
+    bool p1 = false;  // a u-v path inside the SCC's undirected subgraph was found (also a WCC path)
     if (a.twopath) {
         const int32_t gen = a.gen0 + 3;
         const Filter f{a.scc, a.scc[u], nullptr, 0, 0};
         r = bidir(a.sym, a.sym, f, u, v, gen, a.W, S);
+        p1 = r == R_FOUND;
         if (r == R_FOUND) {
             // P1 = u .. m along the forward tree, then m .. v along the backward tree (simple:
             // the search stopped at the first vertex both sides held)
@@ -331,6 +372,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_single_checks(CheckArgs a) {
         }
     }
     if (threadIdx.x == 0) a.out[3] = r;
+    r = R_NOT_RUN;
+    if (a.wcc) {
+        r = p1 ? R_FOUND : bidir(a.sym, a.sym, none, u, v, a.gen0, a.W, S);
+        if (r == R_NONE && a.wcc_label) {
+            const bool fwd_done = S.hi_f == S.lo_f;  // (read by every thread after bidir's barriers)
+            const int n = fwd_done ? S.hi_f : S.hi_b;
+            __syncthreads();
+            wcc_split(a.wcc_label, a.V, a.wcc_label[u], fwd_done ? a.W.q_f : a.W.q_b, n,
+                      fwd_done ? a.W.stamp_f : a.W.stamp_b, a.gen0, S);
+            r = R_SPLIT;
+        }
+    }
+    if (threadIdx.x == 0) a.out[0] = r;
+    r = R_NOT_RUN;
+    if (a.split) {
+        const Filter f{a.scc, a.scc[u], nullptr, 0, 0};
+        r = bidir(a.fw, a.bw, f, u, v, a.gen0 + 1, a.W, S);
+    }
+    if (threadIdx.x == 0) a.out[1] = r;
+    r = R_NOT_RUN;
+    if (a.cycle) {
+        const Filter f{nullptr, 0, a.rank, a.rank[v], a.rank[u]};
+        r = bidir(a.fw, a.bw, f, v, u, a.gen0 + 2, a.W, S);
+    }
+    if (threadIdx.x == 0) a.out[2] = r;
 }
 
 }  // namespace
@@ -366,6 +432,7 @@ int single_op_checks(gir_dev* g, int32_t u, int32_t v, const SingleChecks& want,
     a.sym = view(g->sym);
     a.scc = static_cast<const int32_t*>(g->scc.p);
     a.rank = static_cast<const int32_t*>(g->scc_rank.p);
+    a.wcc_label = want.wcc ? static_cast<int32_t*>(g->wcc.p) : nullptr;
     a.V = V;
     a.u = u;
     a.v = v;

@@ -231,10 +231,11 @@ def test_single_edge_checks_match_oracle(pkg, orc):
     come from the exact device searches, checked against the oracle after every op: deletions of
     existing edges inside SCCs and anywhere, inserts against the rank order (closing a cycle or
     not) and random inserts, on a dense R-MAT (one big SCC and block) and a sparse one (bridges,
-    articulation points, small SCCs). The searches must keep layers many times, and layers must
-    still be patched and rebuilt where the searches say so."""
+    articulation points, small SCCs). The searches must keep layers many times, split weakly
+    connected components in place (the handle's component count follows), and SCCs and blocks
+    must still be patched and rebuilt where the searches say so."""
     seen = {"wcc": set(), "scc": set(), "bct": set()}
-    checked = kept = 0
+    checked = kept = wcc_splits = 0
     for ef, n_ops in ((16, 120), (2, 200)):
         g = pkg.graphs.rmat(11, n_draws=ef << 11, seed=40 + ef, weights=None)
         V = g.V
@@ -263,17 +264,27 @@ def test_single_edge_checks_match_oracle(pkg, orc):
                 u, v, ins = int(rng.integers(V)), int(rng.integers(V)), 1
                 if u == v:
                     continue
+            n_wcc = d.counts()["n_wcc"]
             d.apply_batch(np.array([u], np.int32), np.array([v], np.int32), np.array([ins], np.uint8))
             for k, x in d.batch_plan().items():
                 seen[k].add(x)
+            assert d.counts()["n_wcc"] == len(np.unique(d.labels(pkg.native.LABEL_WCC)))
+            wcc_splits += d.counts()["n_wcc"] > n_wcc
             fb, fa, _, _ = orc.apply_batch(V, fb, fa, [u], [v], [ins])
             _oracle_match(pkg, orc, d, V, fb, fa, f"op {i} ({u} -> {v}, insert {ins}), edge factor {ef}")
+            if i % 40 == 39:  # reachability after the condensation DAG was patched in place
+                srcs = rng.integers(0, V, 6)
+                tgt = rng.integers(0, V, 50).astype(np.int32)
+                for s_ in srcs:
+                    got = d.reachable(np.full(len(tgt), s_, np.int32), tgt)
+                    np.testing.assert_array_equal(got, orc.bfs(V, fb, fa, [int(s_)])[tgt] >= 0)
         st = d.single_stats()
         checked += st["checked"]
         kept += st["kept"]
         d.close()
     assert checked > 100 and kept > 50, (checked, kept)
-    assert {"kept", "rebuilt"} <= seen["wcc"], seen
+    assert wcc_splits > 0
+    assert {"kept", "patched"} <= seen["wcc"], seen
     assert {"kept", "patched", "rebuilt"} <= seen["scc"], seen
     assert {"kept", "rebuilt"} <= seen["bct"], seen
 

@@ -310,7 +310,7 @@ def single_edge_section(pkg, d, ref, n_ops=100):
             res[f"ref_build_{name}_s"] = time.perf_counter() - t
         res["ref_threads"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
     st0 = d.single_stats()
-    dev_ms, plans, phases = [], {"wcc": {}, "scc": {}, "bct": {}}, {0: [], 1: []}
+    dev_ms, plans, phases, per_op = [], {"wcc": {}, "scc": {}, "bct": {}}, {0: [], 1: []}, []
     for a, b, i in ops:
         t = time.perf_counter()
         d.apply_batch(np.array([a], np.int32), np.array([b], np.int32), np.array([i], np.uint8))
@@ -318,8 +318,11 @@ def single_edge_section(pkg, d, ref, n_ops=100):
         ph = d.batch_times()
         ph["checks"] = dev_ms[-1] - sum(ph.values())  # (the searches run between the phases)
         phases[i].append(ph)
-        for k, x in d.batch_plan().items():
+        plan = d.batch_plan()
+        for k, x in plan.items():
             plans[k][x] = plans[k].get(x, 0) + 1
+        # (kind, ms, search ms, decisions as three letters: k kept, p patched, r rebuilt)
+        per_op.append(["id"[i], round(dev_ms[-1], 2), round(ph["checks"], 2), "".join(x[0] for x in plan.values())])
     st1 = d.single_stats()
     by_kind = {}
     for i, name in ((0, "delete"), (1, "insert")):
@@ -329,6 +332,7 @@ def single_edge_section(pkg, d, ref, n_ops=100):
                                              for k in phases[i][0]}}
     res.update(device_median_ms=float(np.median(dev_ms)), device_mean_ms=float(np.mean(dev_ms)),
                device_p90_ms=float(np.percentile(dev_ms, 90)), by_kind=by_kind, layer_decisions=plans,
+               per_op=per_op,
                checked=st1["checked"] - st0["checked"], rebuilds_avoided=st1["kept"] - st0["kept"])
     if ref is not None:
         ref_ms = []

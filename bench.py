@@ -322,7 +322,7 @@ def single_edge_section(pkg, d, ref, n_ops=100):
         for k, x in plan.items():
             plans[k][x] = plans[k].get(x, 0) + 1
         # (kind, ms, search ms, decisions as three letters: k kept, p patched, r rebuilt)
-        per_op.append(["id"[i], round(dev_ms[-1], 2), round(ph["checks"], 2), "".join(x[0] for x in plan.values())])
+        per_op.append(["di"[i], round(dev_ms[-1], 2), round(ph["checks"], 2), "".join(x[0] for x in plan.values())])
     st1 = d.single_stats()
     by_kind = {}
     for i, name in ((0, "delete"), (1, "insert")):

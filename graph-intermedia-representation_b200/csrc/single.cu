@@ -11,13 +11,15 @@
 //  - BCT, the undirected edge {u, v} removed inside an SCC that stays whole: are there still two
 //    internally vertex-disjoint u-v paths in the SCC's undirected subgraph? By Menger's theorem
 //    the block that held {u, v} stays biconnected exactly then, so every block is unchanged.
-//    One path P1 comes from a bidirectional search; the second from one augmenting search in the
-//    residual graph of P1 with every vertex split into an entered and a left state.
+//    One path P1 comes from a bidirectional search. The second is first sought by a plain
+//    bidirectional search around P1's inner vertices (usually enough); only where that finds
+//    none does one augmenting search run in the residual graph of P1, with every vertex split
+//    into an entered and a left state.
 // A WCC split found this way is applied in place (the search that ran out holds the whole new
-// component). All searches run in one CTA of one launch (no host round trip per level) with visited marks
-// stamped by generation, so nothing is cleared between calls, and with budgets on visited
-// vertices and scanned edges: a search that exceeds them reports "unknown" and the layer is
-// rebuilt as before.
+// component). All searches run in one CTA of one launch (no host round trip per level) with
+// visited marks stamped by generation, so nothing is cleared between calls, and with budgets on
+// visited vertices and scanned edges: a search that exceeds them reports "unknown" and the layer
+// is rebuilt as before.
 #include "common.cuh"
 
 namespace gir {
@@ -47,8 +49,15 @@ struct Filter {
     int32_t L;
     const int32_t* rank;  // and rank[x] in [rlo, rhi] (rank null: no rank test)
     int32_t rlo, rhi;
+    const int32_t* pstamp = nullptr;  // and x not inside P1 (stamped pgen at a position in (0, pk))
+    const int32_t* ppos = nullptr;
+    int32_t pgen = 0, pk = 0;
     __device__ bool ok(int32_t x) const {
         if (lab && lab[x] != L) return false;
+        if (pstamp && pstamp[x] == pgen) {
+            const int32_t p = ppos[x];
+            if (p > 0 && p < pk) return false;
+        }
         if (rank) {
             const int32_t r = rank[x];
             return r >= rlo && r <= rhi;
@@ -368,7 +377,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_single_checks(CheckArgs a) {
             __syncthreads();
             const int k = S.tail;
             __syncthreads();
-            r = k > 0 ? second_path(a.sym, f, u, v, k, gen, a.W, S) : R_UNKNOWN;
+            if (k <= 0) {
+                r = R_UNKNOWN;
+            } else {
+                // a path found around P1's inner vertices is disjoint from P1 by construction
+                Filter f2 = f;
+                f2.pstamp = a.W.path_stamp;
+                f2.ppos = a.W.path_pos;
+                f2.pgen = gen;
+                f2.pk = k;
+                r = bidir(a.sym, a.sym, f2, u, v, a.gen0 + 4, a.W, S);
+                if (r != R_FOUND) r = second_path(a.sym, f, u, v, k, gen, a.W, S);
+            }
         }
     }
     if (threadIdx.x == 0) a.out[3] = r;
@@ -443,7 +463,7 @@ int single_op_checks(gir_dev* g, int32_t u, int32_t v, const SingleChecks& want,
     a.gen0 = g->single_gen;
     a.W = W;
     a.out = res;
-    g->single_gen += 4;
+    g->single_gen += 5;
     k_single_checks<<<1, kThreads, 0, g->stream>>>(a);
     GIR_LAUNCH(g, "k_single_checks");
     void* hp = nullptr;

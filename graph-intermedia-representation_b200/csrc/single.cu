@@ -29,7 +29,7 @@ namespace {
 constexpr int kThreads = 1024;
 constexpr int kBigDeg = 512;  // rows longer than this are swept by the whole CTA
 constexpr int kBig = 256;     // deferred long rows per level (overflow: the warp sweeps it)
-constexpr unsigned long long kEdgeBudget = 1ull << 22;
+constexpr unsigned long long kEdgeBudget = 1ull << 20;
 constexpr int kVisitBudget = 1 << 20;
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -81,7 +81,9 @@ struct Shared {
 
 // Expands queue entries [lo, hi) by one level: visit(x, y) for every row entry y of the vertex
 // x = row_of(entry) of every entry (entries with row_of < 0 have no row to sweep). Warps take the
-// short rows; rows longer than kBigDeg are deferred to the whole CTA.
+// short rows; rows longer than kBigDeg are deferred to the whole CTA. The level stops early when
+// the search is over (S.stop) or past its edge budget; the caller then reads the budget first, so
+// a level cut short never counts as a frontier that ran out.
 template <class RowOf, class Visit>
 __device__ void cta_expand(const CSRView& c, const int32_t* q, int lo, int hi, Shared& S, RowOf&& row_of,
                            Visit&& visit) {
@@ -89,7 +91,8 @@ __device__ void cta_expand(const CSRView& c, const int32_t* q, int lo, int hi, S
     if (threadIdx.x == 0) S.nbig = 0;
     __syncthreads();
     for (int i = lo + warp; i < hi; i += nw) {
-        const int stop = __shfl_sync(kFull, ln == 0 ? *(volatile int*)&S.stop : 0, 0);
+        const int stop = __shfl_sync(
+            kFull, ln == 0 ? (*(volatile int*)&S.stop || *(volatile unsigned long long*)&S.edges > kEdgeBudget) : 0, 0);
         if (stop) break;
         const int32_t x = row_of(q[i]);
         if (x < 0) continue;
@@ -110,7 +113,7 @@ __device__ void cta_expand(const CSRView& c, const int32_t* q, int lo, int hi, S
     __syncthreads();
     const int nbig = S.nbig < kBig ? S.nbig : kBig;
     for (int j = 0; j < nbig; ++j) {
-        if (*(volatile int*)&S.stop) break;
+        if (*(volatile int*)&S.stop || *(volatile unsigned long long*)&S.edges > kEdgeBudget) break;
         const int32_t x = S.big[j];
         const int64_t b = c.beg[x];
         const int32_t d = c.deg[x];
@@ -153,12 +156,12 @@ __device__ int bidir(const CSRView& fwd, const CSRView& bwd, const Filter& F, in
     __syncthreads();
     while (true) {
         if (S.stop) break;
-        if (S.hi_f == S.lo_f || S.hi_b == S.lo_b) {
-            if (threadIdx.x == 0) S.result = R_NONE;
+        if (S.edges > kEdgeBudget || S.hi_f + S.hi_b > kVisitBudget) {  // (before the next test)
+            if (threadIdx.x == 0) S.result = R_UNKNOWN;
             break;
         }
-        if (S.edges > kEdgeBudget || S.hi_f + S.hi_b > kVisitBudget) {
-            if (threadIdx.x == 0) S.result = R_UNKNOWN;
+        if (S.hi_f == S.lo_f || S.hi_b == S.lo_b) {
+            if (threadIdx.x == 0) S.result = R_NONE;
             break;
         }
         const bool fside = S.fe <= S.be;
@@ -248,12 +251,12 @@ __device__ int second_path(const CSRView& sym, const Filter& F, int32_t u, int32
     __syncthreads();
     while (true) {
         if (S.stop) break;
-        if (S.hi_f == S.lo_f) {
-            if (threadIdx.x == 0) S.result = R_NONE;
+        if (S.edges > kEdgeBudget || S.hi_f > kVisitBudget) {  // (before the next test)
+            if (threadIdx.x == 0) S.result = R_UNKNOWN;
             break;
         }
-        if (S.edges > kEdgeBudget || S.hi_f > kVisitBudget) {
-            if (threadIdx.x == 0) S.result = R_UNKNOWN;
+        if (S.hi_f == S.lo_f) {
+            if (threadIdx.x == 0) S.result = R_NONE;
             break;
         }
         const int lo = S.lo_f, hi = S.hi_f;

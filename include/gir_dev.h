@@ -274,7 +274,7 @@ int gir_dev_stream(gir_dev_t* g, void** stream);
 int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64_t V, int32_t source, int32_t* level_out,
                         void* stream);
 
-/* ---- learned schedule (north-star "learned part") ---- */
+/* ---- learned schedule ---- */
 
 /* Schedule network: a 2-layer MLP (GIR_SCHED_IN features -> GIR_SCHED_HID tanh -> GIR_SCHED_OUT
  * logits), fp32, trained and evaluated by this library's own CUDA kernels. */

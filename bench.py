@@ -658,7 +658,7 @@ def run_ours(args):
                 "traffic": tr, "kernel": kern, "launches": kl, "kernel_ms": kms,
                 "algorithmic_bytes": kb, "algorithmic_bytes_per_launch": kb / max(kl, 1),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, averaged over one "
-                                  "call (profiles/k_relax_rmat_lj_traffic.md)" if tr else None,
+                                  "call (committed ncu summary under profiles/)" if tr else None,
                 "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"}
 
     # SSSP with the stored U[1,255] weights (the configuration's weights), reported beside

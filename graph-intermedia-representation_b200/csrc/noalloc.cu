@@ -59,16 +59,18 @@ int scratch_for_current_device(int32_t** out) {
     return GIR_OK;
 }
 
-// The CSR is checked before it is used (offsets from 0 to E never decreasing, ids in [0, V)):
-// a bad graph becomes an error status instead of out-of-bounds accesses. cnt[2] = 1 if bad.
-__global__ void k_na_validate(const int64_t* beg, const int32_t* adj, int64_t V, unsigned int* cnt) {
+// The CSR is checked before it is used: beg[0] == 0, offsets never decreasing, beg[V] within the
+// caller's n_adj entries of adj, ids in [0, V). A bad graph becomes an error status instead of
+// out-of-bounds accesses: the id scan never reads past min(beg[V], n_adj). cnt[2] = 1 if bad.
+__global__ void k_na_validate(const int64_t* beg, const int32_t* adj, int64_t n_adj, int64_t V, unsigned int* cnt) {
     const int64_t E = beg[V];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t == 0 && (beg[0] != 0 || E < 0)) atomicExch(&cnt[2], 1u);
+    if (t == 0 && (beg[0] != 0 || E < 0 || E > n_adj)) atomicExch(&cnt[2], 1u);
     for (int64_t v = t; v < V; v += stride)
         if (beg[v] > beg[v + 1]) atomicExch(&cnt[2], 1u);
-    for (int64_t k = t; k < E; k += stride)
+    const int64_t scan = E < 0 ? 0 : (E < n_adj ? E : n_adj);
+    for (int64_t k = t; k < scan; k += stride)
         if (adj[k] < 0 || (int64_t)adj[k] >= V) atomicExch(&cnt[2], 1u);
 }
 
@@ -106,16 +108,38 @@ __global__ void k_na_level(const int64_t* beg, const int32_t* adj, const int32_t
 
 using namespace gir;
 
-extern "C" int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64_t V, int32_t source,
-                                   int32_t* level_out, void* stream) {
+// Device memory the current device can use directly: its own allocations, or managed memory.
+static bool on_current_device(const void* p, int dev) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
+extern "C" int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64_t n_adj, int64_t V,
+                                   int32_t source, int32_t* level_out, void* stream) {
     if (V < 0 || V > GIR_NOALLOC_MAX_V) {
         set_thread_error("bfs_noalloc: V exceeds GIR_NOALLOC_MAX_V (" + std::to_string((long long)GIR_NOALLOC_MAX_V) +
                          " vertices), the size of its static working memory");
         return GIR_ERR_CAPACITY;
     }
+    if (n_adj < 0) {
+        set_thread_error("bfs_noalloc: negative n_adj");
+        return GIR_ERR_INVALID;
+    }
     if (V == 0) return GIR_OK;
-    if (!beg || !adj || !level_out || !is_device_ptr(beg) || !is_device_ptr(level_out) ||
-        !is_device_ptr(adj)) {
+    int cur_dev = 0;
+    if (cudaGetDevice(&cur_dev) != cudaSuccess) {
+        cudaGetLastError();
+        set_thread_error("bfs_noalloc: no current CUDA device");
+        return GIR_ERR_NODEVICE;
+    }
+    if (!on_current_device(beg, cur_dev) || !on_current_device(level_out, cur_dev) ||
+        (n_adj > 0 && !on_current_device(adj, cur_dev))) {
         set_thread_error("bfs_noalloc: beg, adj and level_out must be device memory of the current device");
         return GIR_ERR_INVALID;
     }
@@ -127,11 +151,7 @@ extern "C" int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64
     unsigned int* cnt = reinterpret_cast<unsigned int*>(scratch + 2 * kMaxV);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int dev_sms = 148;
-    {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev);
-    }
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, cur_dev);
     const int grid = dev_sms * 4;
     auto check = [&](cudaError_t e, const char* what) {
         if (e == cudaSuccess) return GIR_OK;
@@ -140,14 +160,14 @@ extern "C" int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64
         return GIR_ERR_CUDA;
     };
     if ((rc = check(cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * kCounters, s), "counter reset"))) return rc;
-    k_na_validate<<<grid, kBlock, 0, s>>>(beg, adj, V, cnt);
+    k_na_validate<<<grid, kBlock, 0, s>>>(beg, adj, n_adj, V, cnt);
     if ((rc = check(cudaGetLastError(), "k_na_validate"))) return rc;
     unsigned int bad = 0;
     if ((rc = check(cudaMemcpyAsync(&bad, cnt + 2, sizeof(bad), cudaMemcpyDeviceToHost, s), "counter read")) ||
         (rc = check(cudaStreamSynchronize(s), "synchronize")))
         return rc;
     if (bad) {
-        set_thread_error("bfs_noalloc: malformed CSR (offsets not monotone from 0, or ids outside [0,V))");
+        set_thread_error("bfs_noalloc: malformed CSR (offsets not monotone from 0, beg[V] beyond n_adj, or ids outside [0,V))");
         return GIR_ERR_MALFORMED;
     }
     k_na_init<<<grid, kBlock, 0, s>>>(level_out, V, source, qa, cnt);

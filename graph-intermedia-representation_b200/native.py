@@ -103,7 +103,7 @@ def dev_lib():
             "gir_dev_sched_train": [_P, _P, _P, _I64, ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_float)],
             "gir_dev_sched_forward": [_P, _P, _I64, _P],
             "gir_dev_sched_grad": [_P, _P, _P, _I64, _P, ctypes.POINTER(ctypes.c_float)],
-            "gir_dev_bfs_noalloc": [_P, _P, _I64, ctypes.c_int32, _P, _P],
+            "gir_dev_bfs_noalloc": [_P, _P, _I64, _I64, ctypes.c_int32, _P, _P],
             "gir_dev_sched_trace": [_P, _P, _P, _I64, ctypes.POINTER(_I64)],
             "gir_dev_sched_delta_choices": [_P],
             "gir_dev_batch_times": [_P, _P],

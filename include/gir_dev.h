@@ -262,17 +262,22 @@ int gir_dev_stream(gir_dev_t* g, void** stream);
  * call time -- a host engine that gives all of a GPU's memory to its own arena, or a
  * latency-critical thread that cannot afford a cudaMalloc / cudaFree (they can synchronize the
  * whole device). It computes the BFS levels of GIR::bfs (gir_query.cpp:108-294) from one source
- * over the caller's compact CSR: beg int64[V+1], adj int32[beg[V]] and level_out int32[V], all in
- * device memory of the current device; `stream` is a cudaStream_t (NULL: the default stream).
+ * over the caller's compact CSR: beg int64[V+1] and adj int32[n_adj] (the allocation's length;
+ * the CSR uses adj[0 .. beg[V])), and writes level_out int32[V]. All three are device memory of
+ * the current device (or managed memory); `stream` is a cudaStream_t (NULL: the default stream).
  * It allocates nothing: its working memory is a static device array sized for at most
  * GIR_NOALLOC_MAX_V vertices (16 MiB, held by every GPU that loads the library until exit);
- * larger V gives GIR_ERR_CAPACITY, a malformed CSR GIR_ERR_MALFORMED (text in
- * gir_dev_last_error(NULL)). The first call on a device looks up that array's device address
- * (cudaGetSymbolAddress): make that first call before any stream capture. All calls share the
- * array: calls that overlap on the GPU (other streams, other threads) race. */
+ * larger V gives GIR_ERR_CAPACITY. The CSR is validated on the device before any level runs and
+ * a bad one gives GIR_ERR_MALFORMED: beg[0] != 0, beg decreasing anywhere, beg[V] > n_adj, or an
+ * id outside [0, V). A source outside [0, V) gives all -1, as GIR::bfs does (gir_query.cpp:112).
+ * Errors leave their text in gir_dev_last_error(NULL). Every BFS level reads one counter back
+ * to the host (a copy and a stream synchronization), so the call costs about one round trip per
+ * level: high-diameter graphs pay for it. The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress): make that first call before any stream capture. All
+ * calls share the array: calls that overlap on the GPU (other streams, other threads) race. */
 #define GIR_NOALLOC_MAX_V (1 << 21)
-int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64_t V, int32_t source, int32_t* level_out,
-                        void* stream);
+int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64_t n_adj, int64_t V, int32_t source,
+                        int32_t* level_out, void* stream);
 
 /* ---- learned schedule ---- */
 

@@ -1,7 +1,9 @@
 """Generates tests/golden/golden.npz from the reference itself.
 
-Run in a container that has the reference sources (the oracle Makefile compiles them into
-oracle/_ref/libgirref.so):  make -C oracle && python tests/golden/make_golden.py
+Run where the reference sources are (the oracle Makefile compiles them into
+oracle/_ref/libgirref.so):
+  make -C oracle REF=<checkout>/gir_constructor && python tests/golden/make_golden.py <checkout>
+(or set GIR_REFERENCE_DIR=<checkout> instead of the argument).
 
 Cases (the reference's own fixtures and known answers, gir_constructor/gir_test.cpp:704-753
 and gir_selftest.cpp:94-233, plus seeded graphs of the self-test's shapes):
@@ -26,7 +28,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle  # noqa: E402
 
-REF_EXAMPLE = "/root/reference/data/example_graph/"
+# The reference's example graph (data/example_graph/ of its checkout), given as the first argument
+# or by the environment variable GIR_REFERENCE_DIR (the checkout's root).
+REF_EXAMPLE = None
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.npz")
 
 
@@ -227,4 +231,8 @@ def main():
 
 
 if __name__ == "__main__":
+    checkout = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GIR_REFERENCE_DIR")
+    if not checkout:
+        sys.exit("usage: make_golden.py <reference checkout> (or set GIR_REFERENCE_DIR)")
+    REF_EXAMPLE = os.path.join(checkout, "data", "example_graph") + os.sep
     main()

@@ -120,6 +120,15 @@ struct gir_dev {
     // Weight-sorted copies of the forward CSR for SSSP ([0] hash weights, [1] stored weights).
     gir::DevCSR ws[2];
     bool ws_valid[2] = {false, false};
+    // SSSP lane order, per weight mode: the distance of every vertex to the vertex of largest
+    // in-degree (uint64[V], UINT64_MAX = does not reach it), from one backward single-lane run.
+    // Queries place sources with close values in neighbouring lanes, so the lanes that share a
+    // 32-byte sector of the distance rows tend to be active in the same bucket. It only orders
+    // lanes, so it is kept across updates (a stale order costs time, never exactness).
+    gir::DevBuf hub_dist[2];
+    bool hub_valid[2] = {false, false};
+    uint64_t hub_max[2] = {0, 0};        // largest finite value of hub_dist
+    bool narrow16_failed[2] = {false, false};  // a 16-bit lane-distance run overflowed on this handle
 
     // Degree bins of the backward CSR (bottom-up traversal): vertex ids by in-degree class.
     gir::DevBuf bins;                // int32[V]: small | medium | large, each ascending
@@ -139,6 +148,8 @@ struct gir_dev {
     gir::DevBuf work[8];              // buffers of the create / batch pipelines (not used by store ops)
     gir::DevBuf lane_dist;            // lane-interleaved SSSP distances (V x lanes)
     gir::DevBuf qitems[5];            // per-queue-entry work items of the SSSP relaxation
+    gir::DevBuf sssp_sets;            // SSSP: every set's source range and lane-order key
+    gir::DevBuf sssp_lanes;           // SSSP: one lane group's source ranges and output rows
     void* pinned = nullptr;           // small pinned host buffer for counters
     size_t pinned_bytes = 0;
 

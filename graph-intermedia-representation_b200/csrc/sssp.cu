@@ -15,6 +15,8 @@
 // Rows are read from a weight-sorted copy of the forward CSR, so a row's light edges are its
 // prefix. Shortest distances are unique, so the result is the same for every Delta, every
 // schedule and every lane grouping.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace gir {
@@ -28,12 +30,18 @@ constexpr uint64_t kInf = ~0ull;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
 // counters: [0] next near queue length, [1] far queue length, [2] settled queue length,
-// [3] min live far distance, [4] far queue length after a split, [5] relaxation items;
+// [3] min live far distance, [4] far queue length after a split, [5] relaxation items,
+// [6] set when a 16-bit lane distance could not hold a tentative distance;
 // accumulated over the call: [16] reached (vertex, lane) pairs, [17] their out-edges
-enum { S_NEAR = 0, S_FAR = 1, S_SET = 2, S_MIN = 3, S_FAR2 = 4, S_ITEMS = 5, S_REACHED = 16, S_EDGES = 17, S_N = 32 };
+enum { S_NEAR = 0, S_FAR = 1, S_SET = 2, S_MIN = 3, S_FAR2 = 4, S_ITEMS = 5, S_OVF = 6, S_REACHED = 16, S_EDGES = 17,
+       S_N = 32 };
 
-__global__ void k_ws_keys(int64_t V, int64_t E, const int64_t* cb, CSRView c, int hash, uint64_t* keys,
-                          uint32_t* cols) {
+// Sort keys (row << 32 | weight) and columns of every entry of the compact copy of `c`. For the
+// forward CSR the weight of entry (u, v) is that of edge u -> v. With `reverse` the rows are
+// those of the backward CSR: row v holds the u of every edge u -> v, whose weight is the hash
+// weight of (u, v) or the stored weight found in the forward row of u (`f`).
+__global__ void k_ws_keys(int64_t V, int64_t E, const int64_t* cb, CSRView c, int hash, int reverse, CSRView f,
+                          uint64_t* keys, uint32_t* cols) {
     GRID_STRIDE(i, E) {
         int64_t lo = 0, hi = V - 1;
         while (lo < hi) {
@@ -43,7 +51,15 @@ __global__ void k_ws_keys(int64_t V, int64_t E, const int64_t* cb, CSRView c, in
         const int64_t u = lo;
         const int64_t p = c.beg[u] + (i - cb[u]);
         const int32_t v = c.adj[p];
-        const uint32_t w = hash ? hash_weight((int32_t)u, v) : c.w[p];
+        uint32_t w;
+        if (!reverse) {
+            w = hash ? hash_weight((int32_t)u, v) : c.w[p];
+        } else if (hash) {
+            w = hash_weight(v, (int32_t)u);
+        } else {
+            const int64_t b = f.beg[v];
+            w = f.w[lower_bound_dev(f.adj, b, b + f.deg[v], (int32_t)u)];
+        }
         keys[i] = ((uint64_t)u << 32) | w;
         cols[i] = (uint32_t)v;
     }
@@ -79,15 +95,14 @@ __global__ void k_deg_i64(int64_t V, const int32_t* deg, int64_t* out) {
     if (blockIdx.x == 0 && threadIdx.x == 0) out[V] = 0;
 }
 
-// Lane s of the group starts at every vertex of set s (set_beg: device copy, absolute offsets).
+// Lane s of the group starts at every vertex of srcs[lane_rng[2s] .. lane_rng[2s + 1]) (one
+// CTA row per lane: blockIdx.y = s).
 template <class D>
-__global__ void k_sssp_init(const int64_t* set_beg, int nl, const int32_t* srcs, int64_t V, D* dist,
+__global__ void k_sssp_init(const int64_t* lane_rng, const int32_t* srcs, int64_t V, int nl, D* dist,
                             unsigned long long* nearmask, int32_t* nearq, unsigned long long* cnt) {
-    const int64_t lo = set_beg[0], hi = set_beg[nl];
-    GRID_STRIDE(i, hi - lo) {
-        const int64_t e = lo + i;
-        int s = 0;
-        while (set_beg[s + 1] <= e) ++s;
+    const int s = blockIdx.y;
+    const int64_t lo = lane_rng[2 * s], hi = lane_rng[2 * s + 1];
+    for (int64_t e = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < hi; e += (int64_t)gridDim.x * blockDim.x) {
         const int32_t v = srcs[e];
         if (v < 0 || v >= V) continue;
         dist[(int64_t)v * nl + s] = 0;
@@ -110,6 +125,27 @@ template <>
 struct DistT<uint32_t> {
     static constexpr uint32_t inf = ~0u;
     __device__ static uint32_t atomic_min(uint32_t* p, uint32_t v) { return atomicMin((unsigned int*)p, v); }
+};
+// 16-bit lane distances (64 lanes in one 128-byte line) when the distances are small: the
+// minimum is taken by compare-and-swap on the aligned 32-bit word holding the lane. Every failed
+// swap means the word changed, and both halves only ever decrease, so the loop ends.
+template <>
+struct DistT<uint16_t> {
+    static constexpr uint16_t inf = 0xffffu;
+    __device__ static uint16_t atomic_min(uint16_t* p, uint16_t v) {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+        unsigned int* wp = reinterpret_cast<unsigned int*>(a & ~(uintptr_t)3);
+        const int sh = (a & 2) ? 16 : 0;
+        unsigned int old = *(volatile unsigned int*)wp;
+        while (true) {
+            const uint16_t cur = (uint16_t)(old >> sh);
+            if (cur <= v) return cur;
+            const unsigned int nw = (old & ~(0xffffu << sh)) | ((unsigned int)v << sh);
+            const unsigned int prev = atomicCAS(wp, old, nw);
+            if (prev == old) return cur;
+            old = prev;
+        }
+    }
 };
 
 // Index of the k-th set bit of a 64-bit mask (k < popcount).
@@ -294,7 +330,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
             uint32_t wt[kPairs];
 #pragma unroll
             for (int j = 0; j < kPairs; ++j) {
-                if (on[j]) { w[j] = a.wadj[k[j]]; wt[j] = a.ww[k[j]]; } else { w[j] = 0; wt[j] = 0; }
+                if (on[j]) { w[j] = __ldcs(&a.wadj[k[j]]); wt[j] = __ldcs(&a.ww[k[j]]); } else { w[j] = 0; wt[j] = 0; }
             }
             uint64_t cur[kPairs];
 #pragma unroll
@@ -305,7 +341,10 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
                 bool to_near = false, to_far = false;
                 if (on[j]) {
                     const uint64_t nd = du[j] + (uint64_t)wt[j];
-                    if (nd < cur[j]) {  // plain pre-check: most relaxations lose
+                    if (sizeof(D) == 2 && nd >= (uint64_t)DistT<D>::inf) {
+                        // a 16-bit lane cannot hold it: the group is run again with 32-bit lanes
+                        if (cur[j] == (uint64_t)DistT<D>::inf) a.cnt[S_OVF] = 1ull;
+                    } else if (nd < cur[j]) {  // plain pre-check: most relaxations lose
                         const uint64_t old = DistT<D>::atomic_min(&dist[(int64_t)w[j] * a.nl + sl[j]], (D)nd);
                         if (nd < old) {
                             const unsigned long long bit = 1ull << sl[j];
@@ -391,9 +430,9 @@ __global__ void k_sssp_reached(const D* dist, int64_t V, int nl, const int32_t* 
     }
 }
 
-// dist[v * nl + s] -> out[s * V + v], through 32 x 32 shared-memory tiles.
+// dist[v * nl + s] -> out[row[s] * V + v], through 32 x 32 shared-memory tiles.
 template <class D>
-__global__ void k_transpose(const D* dist, int64_t V, int nl, uint64_t* out) {
+__global__ void k_transpose(const D* dist, int64_t V, int nl, const int64_t* row, uint64_t* out) {
     __shared__ uint64_t tile[32][33];
     const int64_t v0 = (int64_t)blockIdx.x * 32;
     const int s0 = blockIdx.y * 32;
@@ -410,15 +449,55 @@ __global__ void k_transpose(const D* dist, int64_t V, int nl, uint64_t* out) {
     for (int r = ty; r < 32; r += 8) {
         const int s = s0 + r;
         const int64_t v = v0 + tx;
-        if (v < V && s < nl) out[(int64_t)s * V + v] = tile[tx][r];
+        if (v < V && s < nl) out[row[s] * V + v] = tile[tx][r];
     }
+}
+
+// Lane-order key of every query set: the smallest distance to the hub over the set's sources
+// (UINT64_MAX when none reaches it or none is in range).
+__global__ void k_set_keys(const int64_t* set_beg, int64_t n_sets, const int32_t* srcs, int64_t V,
+                           const uint64_t* hub_dist, uint64_t* key) {
+    GRID_STRIDE(i, n_sets) {
+        uint64_t k = kInf;
+        for (int64_t e = set_beg[i]; e < set_beg[i + 1]; ++e) {
+            const int32_t v = srcs[e];
+            if (v >= 0 && v < V) k = hub_dist[v] < k ? hub_dist[v] : k;
+        }
+        key[i] = k;
+    }
+}
+
+// The vertex of largest in-degree (smallest id among ties) as in-degree << 32 | ~id, and the
+// largest finite value of a distance array: st[0], st[1] (atomicMax).
+__global__ void k_argmax_deg(int64_t V, const int32_t* deg, unsigned long long* st) {
+    unsigned long long best = 0;
+    GRID_STRIDE(v, V) {
+        const unsigned long long k = ((unsigned long long)(uint32_t)deg[v] << 32) | (uint32_t)~(uint32_t)v;
+        best = k > best ? k : best;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+        best = t > best ? t : best;
+    }
+    if (lane_id() == 0) atomicMax(&st[0], best);
+}
+__global__ void k_max_finite(int64_t V, const uint64_t* d, unsigned long long* st) {
+    unsigned long long m = 0;
+    GRID_STRIDE(v, V) if (d[v] != kInf && d[v] > m) m = d[v];
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t > m ? t : m;
+    }
+    if (lane_id() == 0) atomicMax(&st[1], m);
 }
 
 }  // namespace
 
-// Weight-sorted copy of the forward CSR for one weight mode (compact rows).
-static int build_weight_sorted(gir_dev* g, int hash, DevCSR& ws) {
-    const int64_t V = g->V, E = g->fw.E;
+// Weight-sorted compact copy of the forward CSR for one weight mode; with `reverse`, of the
+// backward CSR, each entry (v <- u) carrying the weight of the forward edge u -> v.
+static int build_weight_sorted(gir_dev* g, int hash, int reverse, DevCSR& ws) {
+    const DevCSR& c = reverse ? g->bw : g->fw;
+    const int64_t V = g->V, E = c.E;
     store_free(g, ws);
     uint64_t *keys = nullptr, *ktmp = nullptr;
     uint32_t *cols = nullptr, *ctmp = nullptr;
@@ -428,20 +507,22 @@ static int build_weight_sorted(gir_dev* g, int hash, DevCSR& ws) {
     GIR_TRY(dev_alloc_n(g, &ws.w, E > 0 ? E : 1));
     ws.cap = ws.E = E;
     int64_t* cb = ws.beg;
-    k_deg_i64<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, g->fw.deg, cb);
+    k_deg_i64<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, c.deg, cb);
     GIR_LAUNCH(g, "k_deg_i64");
     GIR_TRY(exclusive_scan_i64(g, cb, cb, V + 1));
-    GIR_CUDA(g, cudaMemcpyAsync(ws.deg, g->fw.deg, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, g->stream));
+    GIR_CUDA(g, cudaMemcpyAsync(ws.deg, c.deg, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, g->stream));
     if (E == 0) return GIR_OK;
     GIR_TRY(ensure_n(g, g->scratch[8], E, &keys));
     GIR_TRY(ensure_n(g, g->scratch[9], E, &ktmp));
     GIR_TRY(ensure_n(g, g->scratch[10], E, &cols));
     GIR_TRY(ensure_n(g, g->scratch[11], E, &ctmp));
-    k_ws_keys<<<grid_for(g, E, kBlock), kBlock, 0, g->stream>>>(V, E, cb, view(g->fw), hash, keys, cols);
+    k_ws_keys<<<grid_for(g, E, kBlock), kBlock, 0, g->stream>>>(V, E, cb, view(c), hash, reverse, view(g->fw), keys,
+                                                                 cols);
     GIR_LAUNCH(g, "k_ws_keys");
     GIR_TRY(sort_pairs_u64(g, keys, ktmp, cols, ctmp, E, 64));
     k_ws_split<<<grid_for(g, E, kBlock), kBlock, 0, g->stream>>>(E, keys, cols, ws.adj, ws.w);
     GIR_LAUNCH(g, "k_ws_split");
+    if (reverse) return GIR_OK;
     // weight statistics for the schedule's features
     unsigned long long* st = reinterpret_cast<unsigned long long*>(ktmp);
     GIR_CUDA(g, cudaMemsetAsync(st, 0, 2 * sizeof(unsigned long long), g->stream));
@@ -455,6 +536,243 @@ static int build_weight_sorted(gir_dev* g, int hash, DevCSR& ws) {
     return GIR_OK;
 }
 
+namespace {
+
+// Working arrays of one SSSP call, sized for V vertices and up to 64 lanes.
+struct Work {
+    int32_t *nearq, *nextq, *farq, *farq2, *setq;
+    unsigned long long *curmask, *nextmask, *farmask, *setmask, *cnt;
+    int4* rows;
+    Items items;
+    unsigned long long* hc;  // pinned host copy of the counters
+};
+
+int sssp_work(gir_dev* g, Work& w) {
+    const int64_t V = g->V;
+    GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &w.nearq));
+    GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &w.nextq));
+    GIR_TRY(ensure_n(g, g->scratch[2], V + 1, &w.farq));
+    GIR_TRY(ensure_n(g, g->scratch[3], V + 1, &w.farq2));
+    GIR_TRY(ensure_n(g, g->scratch[4], V + 1, &w.setq));
+    GIR_TRY(ensure_n(g, g->scratch[5], V + 1, &w.curmask));
+    GIR_TRY(ensure_n(g, g->scratch[6], V + 1, &w.nextmask));
+    GIR_TRY(ensure_n(g, g->scratch[7], V + 1, &w.farmask));
+    GIR_TRY(ensure_n(g, g->scratch[12], V + 1, &w.setmask));
+    GIR_TRY(ensure_n(g, g->scratch[13], S_N, &w.cnt));
+    GIR_TRY(ensure_n(g, g->qitems[3], V + 1, &w.rows));
+    GIR_TRY(ensure_n(g, g->qitems[0], V + 1, &w.items.u));
+    GIR_TRY(ensure_n(g, g->qitems[1], V + 1, &w.items.eb));
+    GIR_TRY(ensure_n(g, g->qitems[2], V + 1, &w.items.m));
+    GIR_TRY(ensure_n(g, g->qitems[4], V + 2, &w.items.pref));
+    void* h = nullptr;
+    GIR_TRY(pinned(g, 256, &h));
+    w.hc = static_cast<unsigned long long*>(h);
+    return GIR_OK;
+}
+
+// One group of nl lanes (1..64) over the weight-sorted rows `ws`: lane s starts from
+// srcs[lane_rng[2s] .. lane_rng[2s + 1]) (device arrays, n_entries sources in all). Lane
+// distances have the type D. With nl == 1 and 64-bit lanes the result is written straight into
+// `out` (V entries); otherwise lane s ends in row lane_row[s] of `out` (rows of V). A 16-bit run
+// that met a distance it cannot hold sets *overflow and writes nothing.
+template <class D>
+int sssp_group(gir_dev* g, Work& wk, const DevCSR& ws, int nl, const int64_t* lane_rng_d, const int32_t* srcs_d,
+               int64_t n_entries, const int64_t* lane_row_d, uint64_t* out, uint64_t Dw, bool* overflow) {
+    const int64_t V = g->V;
+    QueryStats& st = g->qstats;
+    *overflow = false;
+    unsigned long long* cnt = wk.cnt;
+    unsigned long long* hc = wk.hc;
+    auto read = [&]() -> int {
+        GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
+        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+        return GIR_OK;
+    };
+    const bool direct = nl == 1 && sizeof(D) == sizeof(uint64_t);
+    D* dist = nullptr;
+    if (direct) {
+        dist = reinterpret_cast<D*>(out);
+    } else {
+        GIR_TRY(ensure_n(g, g->lane_dist, (size_t)V * nl * sizeof(D) / sizeof(uint64_t) + 1,
+                         reinterpret_cast<uint64_t**>(&dist)));
+    }
+    int per_sm = 0;
+    GIR_CUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_relax<D>, kRelaxThreads, 0));
+    const int run_grid = g->num_sms * (per_sm > 0 ? per_sm : 1);
+    MainTimer timer{g, g->params[GIR_PARAM_PROFILE] != 0.0};
+    int32_t *nearq = wk.nearq, *nextq = wk.nextq, *farq = wk.farq, *farq2 = wk.farq2;
+    unsigned long long *curmask = wk.curmask, *nextmask = wk.nextmask;
+    // (a group that ends on settled-only far entries leaves their lane bits behind)
+    GIR_CUDA(g, cudaMemsetAsync(curmask, 0, sizeof(unsigned long long) * V, g->stream));
+    GIR_CUDA(g, cudaMemsetAsync(nextmask, 0, sizeof(unsigned long long) * V, g->stream));
+    GIR_CUDA(g, cudaMemsetAsync(wk.farmask, 0, sizeof(unsigned long long) * V, g->stream));
+    GIR_CUDA(g, cudaMemsetAsync(wk.setmask, 0, sizeof(unsigned long long) * V, g->stream));
+    GIR_CUDA(g, cudaMemsetAsync(dist, 0xff, sizeof(D) * V * nl, g->stream));
+    for (int k = 0; k < S_N; ++k)
+        if (k != S_REACHED && k != S_EDGES) hc[k] = 0;
+    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, g->stream));
+    if (n_entries > 0) {
+        const int gx = (int)((n_entries / nl + kBlock - 1) / kBlock > 0 ? (n_entries / nl + kBlock - 1) / kBlock : 1);
+        k_sssp_init<D><<<dim3(gx < 1024 ? gx : 1024, nl), kBlock, 0, g->stream>>>(lane_rng_d, srcs_d, V, nl, dist,
+                                                                                  curmask, nearq, cnt);
+        GIR_LAUNCH(g, "k_sssp_init");
+    }
+    GIR_TRY(read());
+    int64_t n_near = (int64_t)hc[S_NEAR], n_far = 0;
+    Relax a;
+    a.wb = ws.beg; a.wdeg = ws.deg; a.wadj = ws.adj; a.ww = ws.w; a.delta = Dw; a.nl = nl; a.dist = dist;
+    a.farmask = wk.farmask; a.setmask = wk.setmask; a.setq = wk.setq; a.cnt = cnt;
+    uint64_t k = 0;
+    int64_t trace_pairs = 0, trace_passes = 0;
+    k_light_split<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, ws.beg, ws.deg, ws.w, Dw, wk.rows);
+    GIR_LAUNCH(g, "k_light_split");
+    Items items = wk.items;
+    // one relaxation pass over queue q (n entries): prep, scan of the work, balanced run
+    auto relax = [&](const int32_t* q, int64_t n, int heavy) -> int {
+        GIR_CUDA(g, cudaMemsetAsync(cnt + S_ITEMS, 0, sizeof(unsigned long long), g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(items.pref, 0, sizeof(int64_t) * (n + 1), g->stream));
+        k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, wk.rows, items);
+        GIR_LAUNCH(g, "k_relax_prep");
+        GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));
+        if (g->trace_marks) {
+            int64_t tot = 0;
+            GIR_CUDA(g, cudaMemcpyAsync(&tot, items.pref + n, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
+            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+            trace_pairs += tot;
+            ++trace_passes;
+        }
+        GIR_TRY(timer.run([&]() -> int {
+            k_relax<D><<<run_grid, kRelaxThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
+            GIR_LAUNCH(g, "k_relax");
+            return GIR_OK;
+        }));
+        st.launches += 4;  // prep, the scan's two kernels, the relaxation
+        return GIR_OK;
+    };
+    while (true) {
+        a.kend = (k + 1) * Dw;
+        GIR_CUDA(g, cudaMemsetAsync(cnt + S_SET, 0, sizeof(unsigned long long), g->stream));
+        // light rounds: nearq (lanes in curmask) -> nextq (lanes in nextmask)
+        while (n_near > 0) {
+            GIR_CUDA(g, cudaMemsetAsync(cnt + S_NEAR, 0, sizeof(unsigned long long), g->stream));
+            a.curmask = curmask; a.nextmask = nextmask; a.nextq = nextq; a.farq = farq;
+            GIR_TRY(relax(nearq, n_near, 0));
+            st.iterations++;
+            std::swap(nearq, nextq);
+            std::swap(curmask, nextmask);
+            GIR_TRY(read());
+            n_near = (int64_t)hc[S_NEAR];
+        }
+        // heavy edges of the (vertex, lane) pairs settled in this bucket
+        const int64_t n_set = (int64_t)hc[S_SET];
+        if (n_set > 0) {
+            a.curmask = curmask; a.nextmask = nextmask; a.nextq = nextq; a.farq = farq;
+            GIR_TRY(relax(wk.setq, n_set, 1));
+        }
+        // next bucket: split the far entries at bucket k + 1; when that one is empty, jump to
+        // the bucket of the smallest distance still far
+        GIR_TRY(read());
+        n_far = (int64_t)hc[S_FAR];
+        if (n_far == 0) break;
+        uint64_t lo = a.kend;
+        bool finished = false;
+        while (true) {
+            k = lo / Dw;
+            GIR_CUDA(g, cudaMemsetAsync(cnt + S_MIN, 0xff, sizeof(unsigned long long), g->stream));
+            GIR_CUDA(g, cudaMemsetAsync(cnt + S_FAR2, 0, sizeof(unsigned long long), g->stream));
+            k_far_split<D><<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(
+                farq, cnt + S_FAR, wk.farmask, dist, nl, k * Dw, (k + 1) * Dw, curmask, nearq, farq2, cnt);
+            GIR_LAUNCH(g, "k_far_split");
+            st.launches++;
+            std::swap(farq, farq2);
+            GIR_CUDA(g, cudaMemcpyAsync(cnt + S_FAR, cnt + S_FAR2, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                        g->stream));
+            GIR_TRY(read());
+            n_near = (int64_t)hc[S_NEAR];
+            n_far = (int64_t)hc[S_FAR];
+            if (n_near > 0) break;
+            if (hc[S_MIN] == kInf) {  // nothing live is left far
+                finished = true;
+                break;
+            }
+            lo = hc[S_MIN];
+        }
+        if (finished) break;
+    }
+    if (g->trace_marks)
+        std::fprintf(stderr, "[gir] sssp group of %d lanes, %d-bit distances, delta %llu: %lld passes, %lld (edge, lane) pairs\n",
+                     nl, (int)(8 * sizeof(D)), (unsigned long long)Dw, (long long)trace_passes, (long long)trace_pairs);
+    if (sizeof(D) == sizeof(uint16_t)) {
+        GIR_TRY(read());
+        if (hc[S_OVF]) {
+            *overflow = true;
+            return GIR_OK;
+        }
+    }
+    k_sssp_reached<D><<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(dist, V, nl, g->fw.deg, cnt);
+    GIR_LAUNCH(g, "k_sssp_reached");
+    if (!direct) {
+        dim3 grd((unsigned)((V + 31) / 32), (unsigned)((nl + 31) / 32));
+        k_transpose<D><<<grd, 256, 0, g->stream>>>(dist, V, nl, lane_row_d, out);
+        GIR_LAUNCH(g, "k_transpose");
+    }
+    return GIR_OK;
+}
+
+}  // namespace
+
+// The lane order of a weight mode (hub_dist, hub_max): one backward single-lane run from the
+// vertex of largest in-degree over a temporary weight-sorted copy of the backward CSR.
+static int hub_order(gir_dev* g, int hash) {
+    const int mi = hash ? 0 : 1;
+    if (g->hub_valid[mi]) return GIR_OK;
+    const int64_t V = g->V;
+    const double t0 = now_ms();
+    const QueryStats saved = g->qstats;
+    uint64_t* hd = nullptr;
+    GIR_TRY(ensure_n(g, g->hub_dist[mi], V, &hd));
+    DevCSR wsb;
+    int rc = build_weight_sorted(g, hash, 1, wsb);
+    Work wk;
+    if (!rc) rc = sssp_work(g, wk);
+    int64_t* lanes = nullptr;
+    if (!rc) rc = ensure_n(g, g->sssp_lanes, 4, &lanes);
+    unsigned long long st[2] = {0, 0};
+    if (!rc) rc = cuda_check(g, cudaMemsetAsync(wk.cnt + 24, 0, 2 * sizeof(unsigned long long), g->stream), "memset");
+    if (!rc) {
+        k_argmax_deg<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, g->bw.deg, wk.cnt + 24);
+        rc = cuda_check(g, cudaGetLastError(), "k_argmax_deg");
+    }
+    if (!rc) rc = cuda_check(g, cudaMemcpyAsync(st, wk.cnt + 24, sizeof(st), cudaMemcpyDeviceToHost, g->stream), "copy");
+    if (!rc) rc = cuda_check(g, cudaStreamSynchronize(g->stream), "sync");
+    if (!rc) {
+        const int32_t hub = (int32_t)~(uint32_t)(st[0] & 0xffffffffull);
+        const int64_t h_lane[2] = {0, 1};
+        int32_t* src_d = reinterpret_cast<int32_t*>(lanes + 2);
+        rc = cuda_check(g, cudaMemcpyAsync(lanes, h_lane, sizeof(h_lane), cudaMemcpyHostToDevice, g->stream), "copy");
+        if (!rc) rc = cuda_check(g, cudaMemcpyAsync(src_d, &hub, sizeof(hub), cudaMemcpyHostToDevice, g->stream), "copy");
+        bool ovf = false;
+        if (!rc) rc = sssp_group<uint64_t>(g, wk, wsb, 1, lanes, src_d, 1, nullptr, hd, 16, &ovf);
+        if (!rc) rc = cuda_check(g, cudaMemsetAsync(wk.cnt + 25, 0, sizeof(unsigned long long), g->stream), "memset");
+        if (!rc) {
+            k_max_finite<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, hd, wk.cnt + 24);
+            rc = cuda_check(g, cudaGetLastError(), "k_max_finite");
+        }
+        if (!rc) rc = cuda_check(g, cudaMemcpyAsync(st, wk.cnt + 24, sizeof(st), cudaMemcpyDeviceToHost, g->stream), "copy");
+        if (!rc) rc = cuda_check(g, cudaStreamSynchronize(g->stream), "sync");
+        if (!rc) {
+            g->hub_max[mi] = st[1];
+            g->hub_valid[mi] = true;
+        }
+    }
+    store_free(g, wsb);
+    g->qstats = saved;
+    if (g->trace_on)
+        std::fprintf(stderr, "[gir] sssp lane order (backward run from the hub, %s weights): %.3f ms, max %llu\n",
+                     hash ? "hash" : "stored", now_ms() - t0, (unsigned long long)g->hub_max[mi]);
+    return rc;
+}
+
 int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_t n_sets, uint64_t delta,
              int weight_mode, uint64_t* dist_d) {
     const int64_t V = g->V;
@@ -466,72 +784,57 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
     GIR_CUDA(g, cudaMemsetAsync(dist_d, 0xff, sizeof(uint64_t) * V * n_sets, g->stream));
     if (V == 0) return GIR_OK;
     const int hash = weight_mode == GIR_WEIGHT_HASH;
+    const int mi = hash ? 0 : 1;
     if (!hash && !g->has_weights) return fail(g, GIR_ERR_STATE, "sssp: the graph has no stored weights");
-    DevCSR& ws = g->ws[hash ? 0 : 1];
-    if (!g->ws_valid[hash ? 0 : 1]) {
-        GIR_TRY(build_weight_sorted(g, hash, ws));
-        g->ws_valid[hash ? 0 : 1] = true;
+    DevCSR& ws = g->ws[mi];
+    if (!g->ws_valid[mi]) {
+        GIR_TRY(build_weight_sorted(g, hash, 0, ws));
+        g->ws_valid[mi] = true;
     }
-    const int64_t nl_max = n_sets < 64 ? n_sets : 64;
-    int32_t *nearq = nullptr, *nextq = nullptr, *farq = nullptr, *farq2 = nullptr, *setq = nullptr;
-    unsigned long long *curmask = nullptr, *nextmask = nullptr, *farmask = nullptr, *setmask = nullptr;
-    unsigned long long* cnt = nullptr;
-    int64_t* sbeg = nullptr;
-    uint64_t* idist = nullptr;
-    GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &nearq));
-    GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &nextq));
-    GIR_TRY(ensure_n(g, g->scratch[2], V + 1, &farq));
-    GIR_TRY(ensure_n(g, g->scratch[3], V + 1, &farq2));
-    GIR_TRY(ensure_n(g, g->scratch[4], V + 1, &setq));
-    GIR_TRY(ensure_n(g, g->scratch[5], V + 1, &curmask));
-    GIR_TRY(ensure_n(g, g->scratch[6], V + 1, &nextmask));
-    GIR_TRY(ensure_n(g, g->scratch[7], V + 1, &farmask));
-    GIR_TRY(ensure_n(g, g->scratch[12], V + 1, &setmask));
-    GIR_TRY(ensure_n(g, g->scratch[13], S_N, &cnt));
-    GIR_TRY(ensure_n(g, g->scratch[14], 65, &sbeg));
-    if (nl_max > 1) GIR_TRY(ensure_n(g, g->lane_dist, (size_t)V * nl_max + 1, &idist));
-    unsigned long long* hc = nullptr;
-    {
-        void* h = nullptr;
-        GIR_TRY(pinned(g, 256, &h));
-        hc = static_cast<unsigned long long*>(h);
-    }
-    auto read = [&]() -> int {
-        GIR_CUDA(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
+    // Lane order: sets sorted by their distance to the hub, so that neighbouring lanes (which
+    // share the 32-byte sectors of a distance row) tend to be active in the same buckets. Only
+    // the placement of the queries changes, never their results.
+    std::vector<int64_t> order((size_t)n_sets);
+    for (int64_t i = 0; i < n_sets; ++i) order[i] = i;
+    if (n_sets > 1) {
+        GIR_TRY(hub_order(g, hash));
+        int64_t* sb = nullptr;
+        GIR_TRY(ensure_n(g, g->sssp_sets, 2 * n_sets + 1, &sb));
+        uint64_t* key_d = reinterpret_cast<uint64_t*>(sb + n_sets + 1);
+        GIR_CUDA(g, cudaMemcpyAsync(sb, set_beg_h, sizeof(int64_t) * (n_sets + 1), cudaMemcpyHostToDevice, g->stream));
+        k_set_keys<<<grid_for(g, n_sets, kBlock), kBlock, 0, g->stream>>>(
+            sb, n_sets, srcs_d, V, static_cast<const uint64_t*>(g->hub_dist[mi].p), key_d);
+        GIR_LAUNCH(g, "k_set_keys");
+        std::vector<uint64_t> key((size_t)n_sets);
+        GIR_CUDA(g, cudaMemcpyAsync(key.data(), key_d, sizeof(uint64_t) * n_sets, cudaMemcpyDeviceToHost, g->stream));
         GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-        return GIR_OK;
-    };
-    const int grid = g->num_sms * (int)g->params[GIR_PARAM_CTAS_PER_SM];
-    MainTimer timer{g, g->params[GIR_PARAM_PROFILE] != 0.0};
-    // the relaxation kernel gives every warp one contiguous run of pairs: one CTA per resident slot
-    int per_sm = 0, per_sm32 = 0;
-    GIR_CUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_relax<uint64_t>, kRelaxThreads, 0));
-    GIR_CUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_relax<uint32_t>, kRelaxThreads, 0));
-    const int run_grid64 = g->num_sms * (per_sm > 0 ? per_sm : 1);
-    const int run_grid32 = g->num_sms * (per_sm32 > 0 ? per_sm32 : 1);
-    // uint32 lane distances when every finite distance fits
-    const double wmax = g->wstat[hash ? 0 : 1][1] > 0 ? g->wstat[hash ? 0 : 1][1] : 4294967295.0;
+        std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return key[x] < key[y]; });
+    }
+    Work wk;
+    GIR_TRY(sssp_work(g, wk));
+    int64_t* lanes = nullptr;  // lane ranges (2 per lane), then output rows (1 per lane)
+    GIR_TRY(ensure_n(g, g->sssp_lanes, 3 * 64, &lanes));
+    // Lane distance width: 32 bits when every finite distance fits ((V - 1) x max weight), else
+    // 64; 16 bits first when the distances to the hub suggest short paths and no 16-bit run of
+    // this handle has overflowed (an overflow reruns the group with the wider type, so the width
+    // never changes a result).
+    const double wmax = g->wstat[mi][1] > 0 ? g->wstat[mi][1] : 4294967295.0;
     const bool fits32 = (double)V * wmax < 4294967295.0;
-    int4* rows = nullptr;
-    GIR_TRY(ensure_n(g, g->scratch[9], V + 1, &rows));
-    Items items;
-    GIR_TRY(ensure_n(g, g->qitems[0], V + 1, &items.u));
-    GIR_TRY(ensure_n(g, g->qitems[1], V + 1, &items.eb));
-    GIR_TRY(ensure_n(g, g->qitems[2], V + 1, &items.m));
-    GIR_TRY(ensure_n(g, g->qitems[4], V + 2, &items.pref));
+    const bool try16 = g->hub_valid[mi] && !g->narrow16_failed[mi] && g->hub_max[mi] * 4 < 0xffffull;
     GIR_CUDA(g, cudaEventRecord(g->ev0, g->stream));
-    GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * S_N, g->stream));
+    GIR_CUDA(g, cudaMemsetAsync(wk.cnt, 0, sizeof(unsigned long long) * S_N, g->stream));
+    std::vector<int64_t> lh(3 * 64);
     for (int64_t g0 = 0; g0 < n_sets; g0 += 64) {
         const int nl = (int)((n_sets - g0) < 64 ? (n_sets - g0) : 64);
-        // (a group that ends on settled-only far entries leaves their lane bits behind)
-        GIR_CUDA(g, cudaMemsetAsync(curmask, 0, sizeof(unsigned long long) * V, g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(nextmask, 0, sizeof(unsigned long long) * V, g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(farmask, 0, sizeof(unsigned long long) * V, g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(setmask, 0, sizeof(unsigned long long) * V, g->stream));
-        const bool narrow = nl > 1 && fits32;  // (one lane writes the uint64 output in place)
-        void* dist = nl > 1 ? (void*)idist : (void*)(dist_d + g0 * V);
-        if (nl > 1)
-            GIR_CUDA(g, cudaMemsetAsync(dist, 0xff, (narrow ? sizeof(uint32_t) : sizeof(uint64_t)) * V * nl, g->stream));
+        int64_t n_entries = 0;
+        for (int j = 0; j < nl; ++j) {
+            const int64_t q = order[g0 + j];
+            lh[2 * j] = set_beg_h[q];
+            lh[2 * j + 1] = set_beg_h[q + 1];
+            lh[2 * nl + j] = q;
+            n_entries += set_beg_h[q + 1] - set_beg_h[q];
+        }
+        GIR_CUDA(g, cudaMemcpyAsync(lanes, lh.data(), sizeof(int64_t) * 3 * nl, cudaMemcpyHostToDevice, g->stream));
         uint64_t D = delta;
         float feat[GIR_SCHED_IN];
         sched_sssp_features(g, weight_mode, nl, feat);
@@ -544,130 +847,25 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
             if (D == 0) D = 16;
         }
         sched_trace(g, feat, sched_delta_class(D));
-        GIR_CUDA(g, cudaMemcpyAsync(sbeg, set_beg_h + g0, sizeof(int64_t) * (nl + 1), cudaMemcpyHostToDevice, g->stream));
-        for (int k = 0; k < S_N; ++k)
-            if (k != S_REACHED && k != S_EDGES) hc[k] = 0;
-        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, g->stream));
-        const int64_t n_entries = set_beg_h[g0 + nl] - set_beg_h[g0];
-        if (n_entries > 0) {
-            if (narrow)
-                k_sssp_init<uint32_t><<<grid_for(g, n_entries, kBlock), kBlock, 0, g->stream>>>(
-                    sbeg, nl, srcs_d, V, static_cast<uint32_t*>(dist), curmask, nearq, cnt);
-            else
-                k_sssp_init<uint64_t><<<grid_for(g, n_entries, kBlock), kBlock, 0, g->stream>>>(
-                    sbeg, nl, srcs_d, V, static_cast<uint64_t*>(dist), curmask, nearq, cnt);
-            GIR_LAUNCH(g, "k_sssp_init");
+        bool ovf = false;
+        if (nl == 1) {
+            GIR_TRY(sssp_group<uint64_t>(g, wk, ws, 1, lanes, srcs_d, n_entries, nullptr, dist_d + order[g0] * V, D, &ovf));
+            continue;
         }
-        GIR_TRY(read());
-        int64_t n_near = (int64_t)hc[S_NEAR], n_far = 0;
-        Relax a;
-        a.wb = ws.beg; a.wdeg = ws.deg; a.wadj = ws.adj; a.ww = ws.w; a.delta = D; a.nl = nl; a.dist = dist;
-        a.farmask = farmask; a.setmask = setmask; a.setq = setq; a.cnt = cnt;
-        uint64_t k = 0;
-        int64_t trace_pairs = 0, trace_passes = 0;
-        // one relaxation pass over queue q (n entries): prep, scan of the work, balanced run
-        k_light_split<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, ws.beg, ws.deg, ws.w, D, rows);
-        GIR_LAUNCH(g, "k_light_split");
-        auto relax = [&](const int32_t* q, int64_t n, int heavy) -> int {
-            GIR_CUDA(g, cudaMemsetAsync(cnt + S_ITEMS, 0, sizeof(unsigned long long), g->stream));
-            GIR_CUDA(g, cudaMemsetAsync(items.pref, 0, sizeof(int64_t) * (n + 1), g->stream));
-            k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, rows, items);
-            GIR_LAUNCH(g, "k_relax_prep");
-            GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));
-            if (g->trace_marks) {
-                int64_t tot = 0;
-                GIR_CUDA(g, cudaMemcpyAsync(&tot, items.pref + n, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
-                GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-                trace_pairs += tot;
-                ++trace_passes;
-            }
-            GIR_TRY(timer.run([&]() -> int {
-                if (narrow)
-                    k_relax<uint32_t><<<run_grid32, kRelaxThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
-                else
-                    k_relax<uint64_t><<<run_grid64, kRelaxThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
-                GIR_LAUNCH(g, "k_relax");
-                return GIR_OK;
-            }));
-            st.launches += 4;  // prep, the scan's two kernels, the relaxation
-            return GIR_OK;
-        };
-        while (true) {
-            a.kend = (k + 1) * D;
-            GIR_CUDA(g, cudaMemsetAsync(cnt + S_SET, 0, sizeof(unsigned long long), g->stream));
-            // light rounds: nearq (lanes in curmask) -> nextq (lanes in nextmask)
-            while (n_near > 0) {
-                GIR_CUDA(g, cudaMemsetAsync(cnt + S_NEAR, 0, sizeof(unsigned long long), g->stream));
-                a.curmask = curmask; a.nextmask = nextmask; a.nextq = nextq; a.farq = farq;
-                GIR_TRY(relax(nearq, n_near, 0));
-                st.iterations++;
-                std::swap(nearq, nextq);
-                std::swap(curmask, nextmask);
-                GIR_TRY(read());
-                n_near = (int64_t)hc[S_NEAR];
-            }
-            // heavy edges of the (vertex, lane) pairs settled in this bucket
-            const int64_t n_set = (int64_t)hc[S_SET];
-            if (n_set > 0) {
-                a.curmask = curmask; a.nextmask = nextmask; a.nextq = nextq; a.farq = farq;
-                GIR_TRY(relax(setq, n_set, 1));
-            }
-            // next bucket: split the far entries at bucket k + 1; when that one is empty, jump to
-            // the bucket of the smallest distance still far
-            GIR_TRY(read());
-            n_far = (int64_t)hc[S_FAR];
-            if (n_far == 0) break;
-            uint64_t lo = a.kend;
-            bool finished = false;
-            while (true) {
-                k = lo / D;
-                GIR_CUDA(g, cudaMemsetAsync(cnt + S_MIN, 0xff, sizeof(unsigned long long), g->stream));
-                GIR_CUDA(g, cudaMemsetAsync(cnt + S_FAR2, 0, sizeof(unsigned long long), g->stream));
-                if (narrow)
-                    k_far_split<uint32_t><<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(
-                        farq, cnt + S_FAR, farmask, static_cast<const uint32_t*>(dist), nl, k * D, (k + 1) * D, curmask,
-                        nearq, farq2, cnt);
-                else
-                    k_far_split<uint64_t><<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(
-                        farq, cnt + S_FAR, farmask, static_cast<const uint64_t*>(dist), nl, k * D, (k + 1) * D, curmask,
-                        nearq, farq2, cnt);
-                GIR_LAUNCH(g, "k_far_split");
-                st.launches++;
-                std::swap(farq, farq2);
-                GIR_CUDA(g, cudaMemcpyAsync(cnt + S_FAR, cnt + S_FAR2, sizeof(unsigned long long),
-                                            cudaMemcpyDeviceToDevice, g->stream));
-                GIR_TRY(read());
-                n_near = (int64_t)hc[S_NEAR];
-                n_far = (int64_t)hc[S_FAR];
-                if (n_near > 0) break;
-                if (hc[S_MIN] == kInf) {  // nothing live is left far
-                    finished = true;
-                    break;
-                }
-                lo = hc[S_MIN];
-            }
-            if (finished) break;
+        const int64_t* rows_d = lanes + 2 * nl;
+        if (try16 && !g->narrow16_failed[mi]) {
+            GIR_TRY(sssp_group<uint16_t>(g, wk, ws, nl, lanes, srcs_d, n_entries, rows_d, dist_d, D, &ovf));
+            if (!ovf) continue;
+            g->narrow16_failed[mi] = true;
+            if (g->trace_on) std::fprintf(stderr, "[gir] sssp: 16-bit lane distances overflowed, group rerun\n");
         }
-        if (g->trace_marks)
-            std::fprintf(stderr, "[gir] sssp group of %d lanes, delta %llu: %lld passes, %lld (edge, lane) pairs\n", nl,
-                         (unsigned long long)D, (long long)trace_passes, (long long)trace_pairs);
-        if (narrow)
-            k_sssp_reached<uint32_t><<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(static_cast<const uint32_t*>(dist),
-                                                                                      V, nl, g->fw.deg, cnt);
+        if (fits32)
+            GIR_TRY(sssp_group<uint32_t>(g, wk, ws, nl, lanes, srcs_d, n_entries, rows_d, dist_d, D, &ovf));
         else
-            k_sssp_reached<uint64_t><<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(static_cast<const uint64_t*>(dist),
-                                                                                      V, nl, g->fw.deg, cnt);
-        GIR_LAUNCH(g, "k_sssp_reached");
-        if (nl > 1) {
-            dim3 grd((unsigned)((V + 31) / 32), (unsigned)((nl + 31) / 32));
-            if (narrow)
-                k_transpose<uint32_t><<<grd, 256, 0, g->stream>>>(static_cast<const uint32_t*>(dist), V, nl, dist_d + g0 * V);
-            else
-                k_transpose<uint64_t><<<grd, 256, 0, g->stream>>>(static_cast<const uint64_t*>(dist), V, nl, dist_d + g0 * V);
-            GIR_LAUNCH(g, "k_transpose");
-        }
+            GIR_TRY(sssp_group<uint64_t>(g, wk, ws, nl, lanes, srcs_d, n_entries, rows_d, dist_d, D, &ovf));
     }
-    GIR_TRY(read());
+    unsigned long long* hc = wk.hc;
+    GIR_CUDA(g, cudaMemcpyAsync(hc, wk.cnt, sizeof(unsigned long long) * S_N, cudaMemcpyDeviceToHost, g->stream));
     GIR_CUDA(g, cudaEventRecord(g->ev1, g->stream));
     GIR_CUDA(g, cudaEventSynchronize(g->ev1));
     st.reached = (int64_t)hc[S_REACHED];

@@ -284,3 +284,41 @@ def test_betweenness_matches_reference(pkg, orc, s16):
         np.testing.assert_allclose(got, exp, rtol=1e-9, atol=1e-9)
         assert exp.max() > 0
         d.close()
+
+
+def test_sssp_lane_order_and_groups_map_back_to_query_rows(pkg, orc, s16):
+    """70 queries (a group of 64 lanes, then 6) with repeats and an out-of-range source: lanes are
+    placed by the sources' distance to the hub, and every lane must land in its own query's row."""
+    g, fb, fa = s16
+    d = pkg.DeviceGraph.from_graph(g)
+    src = pkg.graphs.sources(g.V, 70, 9)
+    src[5] = src[40]
+    src[66] = g.V + 3
+    for weights, w in ((pkg.native.WEIGHT_HASH, None), (pkg.native.WEIGHT_STORED, g.w)):
+        ds = d.sssp(src, delta=16, weights=weights)
+        for i, s in enumerate(src):
+            np.testing.assert_array_equal(ds[i], orc.sssp(g.V, fb, fa, [s], w=w), err_msg=f"query {i}, source {s}")
+    d.close()
+
+
+def test_sssp_16bit_lane_overflow_reruns_wider(pkg, orc):
+    """The distances to the hub are tiny (so 16-bit lane distances are tried first), but a chain of
+    20,000-weight edges holds distances far beyond 65,535: the group must be rerun with wider lanes
+    and still equal the oracle."""
+    V = 200
+    es, ed, ew = [], [], []
+    for i in range(1, 61):
+        es += [i, 0]; ed += [0, i]; ew += [1, 1]
+    es.append(0); ed.append(100); ew.append(1)
+    for i in range(100, 120):
+        es.append(i); ed.append(i + 1); ew.append(20000)
+    g = pkg.graphs.from_edges(V, np.array(es), np.array(ed), np.array(ew, np.uint32))
+    fb, fa = orc.normalize(g.V, g.fw_beg, g.fw_adj)
+    d = pkg.DeviceGraph.from_graph(g)
+    src = np.array([1, 100, 5, 0, 150], np.int32)
+    for _ in range(2):  # the second call starts from the handle's remembered overflow
+        ds = d.sssp(src, delta=16, weights=pkg.native.WEIGHT_STORED)
+        for i, s in enumerate(src):
+            np.testing.assert_array_equal(ds[i], orc.sssp(g.V, fb, fa, [s], w=g.w), err_msg=f"source {s}")
+    assert ds[0, 120] > 65535
+    d.close()

@@ -151,6 +151,67 @@ def canon_blocks(blocks):
     return a[np.lexsort((a[:, 2], a[:, 1], a[:, 0]))]
 
 
+def canon_blocks_csr(beg, verts):
+    """Blocks as a CSR of vertex lists (block i = verts[beg[i]:beg[i+1]]) -> the same sorted
+    (k1, k2, v) triples as canon_blocks, vectorized for millions of blocks (empty blocks are
+    dropped, repeated vertices within a block counted once)."""
+    beg = np.asarray(beg, np.int64)
+    verts = np.asarray(verts, np.int64)
+    nb = len(beg) - 1
+    if nb <= 0 or len(verts) == 0:
+        return np.zeros((0, 3), np.int64)
+    b = np.repeat(np.arange(nb, dtype=np.int64), np.diff(beg))
+    key = np.unique((b << 32) | verts[:len(b)])
+    b, v = key >> 32, key & 0xffffffff
+    starts = np.r_[0, np.nonzero(np.diff(b))[0] + 1]
+    cnt = np.diff(np.r_[starts, len(b)])
+    first = v[starts]
+    second = np.where(cnt > 1, v[np.minimum(starts + 1, len(v) - 1)], -1)
+    idx = np.repeat(np.arange(len(starts)), cnt)
+    t = np.stack([first[idx], second[idx], v], axis=1)
+    return t[np.lexsort((t[:, 2], t[:, 1], t[:, 0]))]
+
+
+def block_forest(V, sb, sa, scc_lab):
+    """The oracle's blocks in the block-cut forest representation the device library returns
+    (v_block / blk_parent_ap / v_bcnt, gir_constructor/gir.h:420-423): every vertex labelled with
+    one block, every block headed by the articulation point through which it hangs off its
+    parent block (-1 for the root block of an SCC), and the number of blocks holding each vertex.
+    Blocks are walked breadth-first from the block of each SCC's smallest vertex. Small graphs
+    only (Python loops)."""
+    t = bicc(V, sb, sa, scc_lab)[0]
+    blocks = {}
+    for k1, k2, v in t:
+        blocks.setdefault((int(k1), int(k2)), []).append(int(v))
+    blist = sorted(blocks.values(), key=lambda b: min(b))
+    of = {}
+    for i, b in enumerate(blist):
+        for v in b:
+            of.setdefault(v, []).append(i)
+    nb = len(blist)
+    label = np.full(V, -1, np.int64)
+    head = np.full(nb, -2, np.int64)
+    bcnt = np.zeros(V, np.int64)
+    for v, bs in of.items():
+        bcnt[v] = len(bs)
+    for r in range(nb):
+        if head[r] != -2:
+            continue
+        head[r] = -1
+        queue = [r]
+        while queue:
+            b = queue.pop(0)
+            for v in blist[b]:
+                if v == head[b]:
+                    continue
+                label[v] = b
+                for c in of[v]:
+                    if head[c] == -2:
+                        head[c] = v
+                        queue.append(c)
+    return label.astype(np.int32), head.astype(np.int32), bcnt.astype(np.int32)
+
+
 def canon_blocks_from_device(label_block, head):
     """Device representation (block of every vertex + head AP of every block) -> triples."""
     label_block = np.asarray(label_block, np.int64)
@@ -440,7 +501,7 @@ class RefGIR:
         beg = np.zeros(nbk.value + 1, np.int64)
         verts = np.zeros(max(n, 1), np.int32)
         ref().ref_blocks(self.h, ptr(beg), ptr(verts), ctypes.byref(nbk))
-        return canon_blocks(verts[beg[i]:beg[i + 1]] for i in range(nbk.value))
+        return canon_blocks_csr(beg, verts[:n])
 
     def ap(self):
         out = np.zeros(max(self.V, 1), np.uint8)

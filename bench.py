@@ -282,7 +282,45 @@ def reference_instance(pkg, d):
                  "input": f"int32 four-array CSR of the current graph (V={d.V}, E={len(ca)}), host memory"}
 
 
-def single_edge_section(pkg, d, ref, n_ops=100):
+def cpu_model():
+    """The host CPU's model name and logical core count."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return f"{line.split(':', 1)[1].strip()} ({os.cpu_count()} logical cores)"
+    except OSError:
+        pass
+    return f"unknown ({os.cpu_count()} logical cores)"
+
+
+def parity_vs_reference(pkg, d, ref, native, n_src=4):
+    """Bit-exactness of the device's layers and queries against the reference on the same graph
+    (canonical forms): WCC, SCC, condensation-DAG key set, blocks, articulation points, BFS levels
+    and SSSP distances (delta 16, hash weights) from n_src sources each."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    t0 = time.perf_counter()
+    res = {"wcc": bool(np.array_equal(d.labels(native.LABEL_WCC), ref.wcc())),
+           "scc": bool(np.array_equal(d.labels(native.LABEL_SCC), ref.scc()))}
+    s, t = d.dag()
+    res["dag"] = bool(np.array_equal(np.unique((s.astype(np.int64) << 32) | t.astype(np.int64)), ref.dag()))
+    label, head = d.blocks()
+    res["blocks"] = bool(np.array_equal(oracle.canon_blocks_from_device(label, head), ref.blocks()))
+    res["articulation_points"] = bool(np.array_equal(d.labels(native.LABEL_BCNT) >= 2, ref.ap()))
+    fb, fa = d.csr(0)
+    src = pkg.graphs.sources_with_edges(pkg.graphs.Graph(d.V, fb.astype(np.int32), fa, None, None), n_src, 17)
+    lv = d.bfs(src)
+    ds = d.sssp(src, delta=DELTA, weights=native.WEIGHT_HASH)
+    res["bfs_rows"] = bool(all(np.array_equal(lv[i], ref.bfs(int(x))) for i, x in enumerate(src)))
+    res["sssp_rows"] = bool(all(np.array_equal(ds[i], ref.sssp(int(x), DELTA)) for i, x in enumerate(src)))
+    res["state"] = "after the build and the 10K, 100K and 1M-edge batches of updates_per_s"
+    res["check_s"] = time.perf_counter() - t0
+    return res
+
+
+def single_edge_section(pkg, d, ref, ref_builds, n_ops=100):
     """Single-edge updates (insertEdge / deleteEdge, gir.cpp:3043-3134) on the current graph with
     every layer kept exact: n_ops ops alternating between deleting an existing edge and inserting
     a random pair, one call each, host wall clock per call (the call returns after the device is
@@ -304,10 +342,7 @@ def single_edge_section(pkg, d, ref, n_ops=100):
             ops.append((a, b if b != a else (a + 1) % V, 1))
     res = {"ops": n_ops}
     if ref is not None:
-        for mask, name in ((1, "wcc"), (2, "scc_dag"), (4, "bct")):
-            t = time.perf_counter()
-            ref.build(mask)
-            res[f"ref_build_{name}_s"] = time.perf_counter() - t
+        res.update(ref_builds)  # the reference's layers were built before the update batches
         res["ref_threads"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
     st0 = d.single_stats()
     dev_ms, plans, phases, per_op = [], {"wcc": {}, "scc": {}, "bct": {}}, {0: [], 1: []}, []
@@ -692,6 +727,18 @@ def run_ours(args):
         rep = None
         if world > 1:  # replicas: rank 0's batch is broadcast, so every replica stays identical
             rep = importlib.import_module("graph-intermedia-representation_b200.replicas").Replicas(d)
+        # the reference on the host cores, holding the same graph (create timed beside the
+        # device's), its three layers built; it takes the same batches, timed beside the device's
+        ref, ref_builds = None, {}
+        if rank == 0 and world == 1 and not args.no_cpu:
+            os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+            ref, extra["create_from_csr"] = reference_instance(pkg, d)
+            if ref is not None:
+                for mask, name in ((1, "wcc"), (2, "scc_dag"), (4, "bct")):
+                    t0 = time.perf_counter()
+                    ref.build(mask)
+                    ref_builds[f"ref_build_{name}_s"] = time.perf_counter() - t0
+        upd_ref = {}
         for n in (10_000, 100_000, 1_000_000):
             if rep is not None:
                 u, v, ins = rep.broadcast_batch(*(pkg.graphs.updates(g, n // 2, n // 2, 50 + n) if rank == 0 else ()))
@@ -701,7 +748,18 @@ def run_ours(args):
             t = ev_time(stream, lambda: d.apply_batch(ub.numpy(), vb.numpy(), ib.numpy()))
             upd[str(n)] = n / (t * 1e-3)
             extra.setdefault("update_phases_ms", {})[str(n)] = {k: round(x, 2) for k, x in d.batch_times().items()}
+            extra.setdefault("update_plans", {})[str(n)] = d.batch_plan()
+            if ref is not None:
+                t0 = time.perf_counter()
+                ref.apply_batch(u, v, ins)
+                upd_ref[str(n)] = n / (time.perf_counter() - t0)
         extra["updates_per_s"] = upd
+        if ref is not None:
+            extra["updates_per_s_reference"] = {
+                "value": upd_ref, "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())),
+                "cpu": cpu_model(), "note": "GIR::applyBatch of the reference compiled from its sources, the same "
+                                            "batches on the same graph, host wall clock"}
+            extra["full_size_parity"] = parity_vs_reference(pkg, d, ref, native)
         # reachability (GIR::reachable) for 64K random pairs on the current graph, device arrays
         n_r = 1 << 16
         rng = np.random.default_rng(77)
@@ -714,14 +772,10 @@ def run_ours(args):
         bc_out = torch.empty(V, dtype=torch.float64, device=dev)
         t_bc = ev_time(stream, lambda: d.bc(sb_d, out=bc_out))
         extra["bc_64_sources_ms"] = t_bc
-        # the reference on the host cores, holding the same graph (create timed beside the device's)
-        ref = None
-        if rank == 0 and world == 1 and not args.no_cpu:
-            ref, extra["create_from_csr"] = reference_instance(pkg, d)
         # single-edge update latency (every layer kept exact), beside the reference's; first, since
         # the reference's single-edge entry points sync the batches ingestBatch leaves pending
         if not args.no_single:
-            extra["single_edge_updates"] = single_edge_section(pkg, d, ref)
+            extra["single_edge_updates"] = single_edge_section(pkg, d, ref, ref_builds)
         # incremental BFS / SSSP of one source under 1K / 10K / 100K-op batches
         if not args.no_incremental:
             extra["incremental"] = incremental_section(pkg, d, stream, dev, int(sb_d[0].item()), ref)

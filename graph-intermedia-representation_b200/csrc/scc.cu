@@ -6,7 +6,8 @@
 // (as in iSpan / Multistep, gir_constructor/includes/scc_cpu):
 //  1. trim-1 as a worklist: a vertex without an in- or out-neighbour among the unassigned
 //     vertices (self-loops ignored) is a singleton SCC; removing it lowers its neighbours'
-//     counts, which may trim them in turn;
+//     counts, which may trim them in turn; then trim-2: two vertices that are each other's only
+//     unassigned in- (or out-) neighbour form an SCC of two;
 //  2. forward-backward from a pivot of maximal out-degree x in-degree (the giant SCC of a
 //     power-law graph): SCC(pivot) = forward reach ∩ backward reach over unassigned vertices;
 //  3. colour propagation for the rest, repeated until every vertex is assigned: every
@@ -77,6 +78,43 @@ __global__ void __launch_bounds__(kBlock) k_trim_in(const int32_t* q, const unsi
         if (atomicSub(&outdeg[w], 1) == 1) return atomicCAS(&label[w], -1, w) == -1;
         return false;
     });
+}
+
+// Trim-2 (iSpan's trim_2_from_fq, gir_constructor/includes/scc_cpu/trim_2_3.h:161, as an
+// algorithm source): u and v form an SCC of two when each is the other's only unassigned in-
+// neighbour (or, in the second pass, only unassigned out-neighbour): no other unassigned vertex
+// reaches either, and the two edges close the cycle. Two launches per direction, so labels are
+// never read while they change: k_trim2_pair records each vertex's only unassigned neighbour in
+// rows `c` when its count (`deg_act`, exact or an over-count of the unassigned neighbours) is 1,
+// then k_trim2_apply labels the mutual pairs with the smaller id.
+__global__ void k_trim2_pair(int64_t V, CSRView c, const int32_t* label, const int32_t* deg_act, int32_t* partner) {
+    GRID_STRIDE(u, V) {
+        int32_t p = -1;
+        if (label[u] == -1 && deg_act[u] == 1) {
+            const int64_t b = c.beg[u], e = b + c.deg[u];
+            for (int64_t k = b; k < e; ++k) {
+                const int32_t w = c.adj[k];
+                if (w != (int32_t)u && label[w] == -1) {
+                    p = w;
+                    break;
+                }
+            }
+        }
+        partner[u] = p;
+    }
+}
+
+__global__ void k_trim2_apply(int64_t V, const int32_t* partner, int32_t* label, unsigned long long* n_pairs) {
+    unsigned long long c = 0;
+    GRID_STRIDE(u, V) {
+        const int32_t p = partner[u];
+        if (p >= 0 && partner[p] == (int32_t)u) {
+            label[u] = p < (int32_t)u ? p : (int32_t)u;
+            c += p > (int32_t)u;
+        }
+    }
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane_id() == 0 && c) atomicAdd(n_pairs, c);
 }
 
 // Pivot: the unassigned vertex with the largest out x in degree (ties: larger id).
@@ -336,6 +374,24 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
         GIR_LAUNCH(g, "k_trim_in");
         return GIR_OK;
     }));
+
+    // trim-2: SCCs of two vertices, through in-neighbours, then through out-neighbours
+    {
+        int32_t* partner = color;  // (colours are set up later)
+        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+        for (int dir = 0; dir < 2; ++dir) {
+            k_trim2_pair<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, dir ? fw : bw, label, dir ? outdeg : indeg,
+                                                                           partner);
+            GIR_LAUNCH(g, "k_trim2_pair");
+            k_trim2_apply<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, partner, label, &cnt[C_ROOTS]);
+            GIR_LAUNCH(g, "k_trim2_apply");
+        }
+        if (g->trace_marks) {
+            GIR_CUDA(g, cudaMemcpyAsync(lp.hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+            std::fprintf(stderr, "[gir] scc: trim-2 pairs %llu\n", (unsigned long long)lp.hc[C_ROOTS]);
+        }
+    }
 
     trace_mark(g, "scc: trim");
     // 2. forward-backward from the max-degree pivot

@@ -147,7 +147,8 @@ def test_rmat_s16_layers_and_batches(pkg, orc, s16):
 
 def test_shapes_high_diameter_and_dense(pkg, orc):
     """A long directed cycle (one SCC, deep BFS tree, no AP), a path of 2-cycles (every inner
-    vertex an AP), a lattice (symmetric, many blocks) and a dense random graph."""
+    vertex an AP), a lattice (symmetric, many blocks), a dense random graph, and 2-cycles with
+    self-loops, some closed and some tied into larger SCCs (trim-2)."""
     cases = []
     n = 3000
     cases.append(("cycle", n, np.arange(n), (np.arange(n) + 1) % n))
@@ -159,10 +160,18 @@ def test_shapes_high_diameter_and_dense(pkg, orc):
     cases.append(("lattice", lat.V, rows, lat.fw_adj))
     rng = np.random.default_rng(5)
     cases.append(("dense", 500, rng.integers(0, 500, 20000), rng.integers(0, 500, 20000)))
+    # 2-cycles (the trim-2 case): 500 pairs, some closed, others tied to the rest by one-way
+    # edges or merged into larger SCCs by random edges, several with self-loops
+    p = np.arange(500)
+    rs, rt = rng.integers(0, 1000, 350), rng.integers(0, 1000, 350)
+    loops = rng.integers(0, 1000, 40)
+    ring = np.arange(30)  # pairs 0..30 chained into one SCC of 62 vertices
+    cases.append(("pairs", 1000, np.concatenate([2 * p, 2 * p + 1, rs, loops, 2 * ring + 1, [61]]),
+                  np.concatenate([2 * p + 1, 2 * p, rt, loops, 2 * ring + 2, [0]])))
     for name, V, s, t in cases:
         s = np.asarray(s, np.int32)
         t = np.asarray(t, np.int32)
-        keep = s != t
+        keep = (s != t) | (name == "pairs")
         gg = pkg.graphs.from_edges(V, s[keep], t[keep])
         d = pkg.DeviceGraph.from_graph(gg, weights=False)
         d.build(pkg.native.LAYER_ALL)

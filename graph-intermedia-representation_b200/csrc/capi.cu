@@ -398,11 +398,34 @@ int rebuild_layers(gir_dev* g, const RepairPlan& plan) {
     return GIR_OK;
 }
 
+// sync (gir.cpp:3602-3632): the layers catch up with every batch ingested since the last sync,
+// in one repair whose plan joins what each of those batches could change.
+int sync_impl(gir_dev* g) {
+    if (!g->pend) return GIR_OK;
+    RepairPlan plan;
+    plan.wcc = g->pend_wcc_del ? REBUILD : (g->n_pend_pairs > 0 ? PATCH : KEEP);
+    plan.pairs_in = static_cast<const uint64_t*>(g->pend_pairs.p);
+    plan.n_pairs_in = g->n_pend_pairs;
+    plan.scc = (g->pend_scc_split || g->pend_scc_cycle) ? REBUILD : (g->pend_dag ? PATCH : KEEP);
+    plan.bct = g->pend_bct ? REBUILD : KEEP;
+    for (double& x : g->b_ms) x = 0;
+    g->b_plan[0] = plan.wcc;
+    g->b_plan[1] = plan.scc;
+    g->b_plan[2] = plan.scc == REBUILD ? REBUILD : plan.bct;
+    GIR_TRY(rebuild_layers(g, plan));
+    g->pend = g->pend_scc_split = g->pend_scc_cycle = g->pend_dag = g->pend_bct = g->pend_wcc_del = false;
+    g->n_pend_pairs = 0;
+    return GIR_OK;
+}
+
 // Filter-Merge-Update on the device (applyBatch, gir.cpp:3634-4111): normalise the batch,
 // merge it into the forward, backward and symmetrized slack CSRs, then bring every built layer
-// up to date.
-int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n) {
+// up to date. With `deferred` (ingestBatch, gir.cpp:3588-3596) the layers are left as they are
+// and what the batch can change is added to the pending plan for the next sync; otherwise
+// pending batches are synced first, as the reference's applyBatch does.
+int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n, bool deferred) {
     const int64_t V = g->V;
+    if (!deferred) GIR_TRY(sync_impl(g));
     g->b_ins = g->b_del = g->b_noop = g->b_invalid = 0;
     for (double& x : g->b_ms) x = 0;
     for (int& x : g->b_plan) x = 0;  // (a batch without effective ops keeps every layer)
@@ -533,6 +556,32 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     GIR_CUDA(g, cudaMemcpyAsync(fl, cnt, sizeof(fl), cudaMemcpyDeviceToHost, g->stream));
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     g->b_ms[0] = now_ms() - t_start;
+    if (deferred) {
+        g->pend = true;
+        g->pend_wcc_del |= nsd > 0;
+        g->pend_scc_split |= fl[F_SCC_SPLIT] != 0;
+        g->pend_scc_cycle |= fl[F_SCC_CYCLE] != 0;
+        g->pend_dag |= fl[F_DAG] != 0;
+        g->pend_bct |= fl[F_BCT] != 0;
+        if (nsi > 0 && g->wcc_built) {
+            uint64_t* keep = nullptr;
+            const size_t need = (size_t)(g->n_pend_pairs + nsi);
+            if (g->pend_pairs.bytes < need * sizeof(uint64_t) + 16) {  // grow, keeping the pairs so far
+                DevBuf nb;
+                GIR_TRY(ensure_n(g, nb, 2 * need, &keep));
+                if (g->n_pend_pairs)
+                    GIR_CUDA(g, cudaMemcpyAsync(keep, g->pend_pairs.p, sizeof(uint64_t) * g->n_pend_pairs,
+                                                cudaMemcpyDeviceToDevice, g->stream));
+                release(g, g->pend_pairs);
+                g->pend_pairs = nb;
+            }
+            keep = static_cast<uint64_t*>(g->pend_pairs.p);
+            GIR_CUDA(g, cudaMemcpyAsync(keep + g->n_pend_pairs, sym_ins, sizeof(uint64_t) * nsi, cudaMemcpyDeviceToDevice,
+                                        g->stream));
+            g->n_pend_pairs += nsi;
+        }
+        return GIR_OK;
+    }
     RepairPlan plan;
     plan.wcc = nsd > 0 ? REBUILD : (nsi > 0 ? PATCH : KEEP);
     plan.pairs_in = sym_ins;
@@ -707,7 +756,7 @@ int gir_dev_destroy(gir_dev_t* g) {
         store_free(g, g->ws[0]); store_free(g, g->ws[1]);
         for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->dag_rows, &g->reach_hub, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
                           &g->cub_tmp, &g->stage_in, &g->stage_out, &g->sched_w, &g->sched_io, &g->lane_dist, &g->inc_st[0], &g->inc_st[1],
-                          &g->inc_pend[0], &g->inc_pend[1], &g->single_ws, &g->hub_dist[0], &g->hub_dist[1], &g->sssp_sets, &g->sssp_lanes})
+                          &g->inc_pend[0], &g->inc_pend[1], &g->single_ws, &g->hub_dist[0], &g->hub_dist[1], &g->sssp_sets, &g->sssp_lanes, &g->pend_pairs})
             release(g, *b);
         for (auto& b : g->scratch) release(g, b);
         for (auto& b : g->work) release(g, b);
@@ -743,6 +792,7 @@ int gir_dev_counts(gir_dev_t* g, int64_t* V, int64_t* E, int64_t* n_wcc, int64_t
 int gir_dev_build(gir_dev_t* g, unsigned layers) {
     if (!g) return GIR_ERR_INVALID;
     if (layers & ~7u) return fail(g, GIR_ERR_INVALID, "gir_dev_build: unknown layer bits");
+    GIR_TRY(sync_impl(g));  // (the layers built so far catch up with ingested batches first)
     if (layers & GIR_LAYER_WCC) GIR_TRY(wcc_build(g));
     if (layers & GIR_LAYER_SCC) GIR_TRY(scc_build(g));
     if (layers & GIR_LAYER_BCT) {
@@ -944,6 +994,7 @@ int gir_dev_reachable(gir_dev_t* g, const int32_t* u, const int32_t* v, int64_t 
     if (n < 0 || (n > 0 && (!u || !v || !out))) return fail(g, GIR_ERR_INVALID, "reachable: bad arguments");
     if (!g->scc_built) return fail(g, GIR_ERR_STATE, "reachable needs buildSCC_DAG first");
     if (n == 0) return GIR_OK;
+    GIR_TRY(sync_impl(g));  // a structure-based query: ingested batches are synced first (gir.h:107-113)
     DevBuf su, sv;
     const void *du = nullptr, *dv = nullptr;
     void* dout = nullptr;
@@ -982,9 +1033,30 @@ int gir_dev_sssp_sets(gir_dev_t* g, const int64_t* set_beg, const int32_t* set_s
 int gir_dev_apply_batch(gir_dev_t* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n) {
     if (!g) return GIR_ERR_INVALID;
     if (n < 0 || (n > 0 && (!u || !v || !ins))) return fail(g, GIR_ERR_INVALID, "apply_batch: bad arguments");
-    const int rc = apply_batch_impl(g, u, v, ins, n);
+    const int rc = apply_batch_impl(g, u, v, ins, n, false);
     release_scratch(g, kKeepScratchBelow);
     return rc;
+}
+
+int gir_dev_ingest_batch(gir_dev_t* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n) {
+    if (!g) return GIR_ERR_INVALID;
+    if (n < 0 || (n > 0 && (!u || !v || !ins))) return fail(g, GIR_ERR_INVALID, "ingest_batch: bad arguments");
+    const int rc = apply_batch_impl(g, u, v, ins, n, true);
+    release_scratch(g, kKeepScratchBelow);
+    return rc;
+}
+
+int gir_dev_sync(gir_dev_t* g) {
+    if (!g) return GIR_ERR_INVALID;
+    const int rc = sync_impl(g);
+    release_scratch(g, kKeepScratchBelow);
+    return rc;
+}
+
+int gir_dev_synced(gir_dev_t* g, int* out) {
+    if (!g || !out) return GIR_ERR_INVALID;
+    *out = g->pend ? 0 : 1;
+    return GIR_OK;
 }
 
 int gir_dev_set_weight_rule(gir_dev_t* g, uint64_t seed, uint32_t lo, uint32_t hi) {

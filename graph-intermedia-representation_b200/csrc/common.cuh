@@ -153,6 +153,16 @@ struct gir_dev {
     void* pinned = nullptr;           // small pinned host buffer for counters
     size_t pinned_bytes = 0;
 
+    // Deferred maintenance (GIR::ingestBatch / sync, gir.h:107-116): batches ingested since the
+    // last sync are in the edge store already; the layers still describe the last sync. What the
+    // pending changes can do to each layer is accumulated (flags judged against the labels of the
+    // last sync, OR-ed over the ingested batches) with the undirected pairs they made present, so
+    // that sync repairs the layers once for all of them.
+    bool pend = false;
+    bool pend_scc_split = false, pend_scc_cycle = false, pend_dag = false, pend_bct = false, pend_wcc_del = false;
+    gir::DevBuf pend_pairs;          // uint64 keys of undirected pairs made present
+    int64_t n_pend_pairs = 0;
+
     // Batch statistics
     int64_t b_ins = 0, b_del = 0, b_noop = 0, b_invalid = 0;
     double b_ms[4] = {0, 0, 0, 0};    // phases of the last batch: store, WCC, SCC, BCT

@@ -2,6 +2,7 @@
 #include "gir_b200.hpp"
 
 #include <algorithm>
+#include <cstdio>
 #include <utility>
 
 namespace gir_b200 {
@@ -70,6 +71,95 @@ GIR GIR::fromEdges(int V, const std::vector<std::pair<int, int>>& edges) {
     return GIR(V, fb, fa, bb, ba);
 }
 
+graph::graph(const char* fw_beg_file, const char* fw_csr_file, const char* bw_beg_file, const char* bw_csr_file) {
+    auto read_all = [](const char* path, std::vector<int32_t>& out) {
+        FILE* f = std::fopen(path, "rb");
+        if (!f) throw Error(GIR_ERR_FILE, std::string(path) + " cannot open");
+        std::fseek(f, 0, SEEK_END);
+        const long bytes = std::ftell(f);
+        std::fseek(f, 0, SEEK_SET);
+        if (bytes < 0 || bytes % 4) {
+            std::fclose(f);
+            throw Error(GIR_ERR_FILE, std::string(path) + " is not an int32 array");
+        }
+        out.resize((size_t)bytes / 4);
+        const size_t got = out.empty() ? 0 : std::fread(out.data(), 4, out.size(), f);
+        std::fclose(f);
+        if (got != out.size()) throw Error(GIR_ERR_FILE, std::string(path) + " is short");
+    };
+    std::vector<int32_t> fb, fa, bb, ba;
+    read_all(fw_beg_file, fb);
+    read_all(fw_csr_file, fa);
+    read_all(bw_beg_file, bb);
+    read_all(bw_csr_file, ba);
+    // graph.cpp:95-114: sizes agree, offsets monotone from 0 to E, ids in [0, V)
+    if (fb.empty() || fb.size() != bb.size() || fa.size() != ba.size())
+        throw Error(GIR_ERR_MALFORMED, "graph: four-file sizes disagree");
+    const int64_t V = (int64_t)fb.size() - 1, E = (int64_t)fa.size();
+    auto ok = [&](const std::vector<int32_t>& beg, const std::vector<int32_t>& adj) {
+        if (beg[0] != 0 || beg[V] != E) return false;
+        for (int64_t i = 0; i < V; ++i)
+            if (beg[i] > beg[i + 1]) return false;
+        for (int32_t x : adj)
+            if (x < 0 || x >= V) return false;
+        return true;
+    };
+    if (!ok(fb, fa) || !ok(bb, ba)) throw Error(GIR_ERR_MALFORMED, "graph: malformed CSR");
+    vert_count = (index_t)V;
+    edge_count = (index_t)E;
+    fw_beg_pos = new index_t[V + 1];
+    bw_beg_pos = new index_t[V + 1];
+    fw_csr = new vertex_t[E > 0 ? E : 1];
+    bw_csr = new vertex_t[E > 0 ? E : 1];
+    std::copy(fb.begin(), fb.end(), fw_beg_pos);
+    std::copy(bb.begin(), bb.end(), bw_beg_pos);
+    std::copy(fa.begin(), fa.end(), fw_csr);
+    std::copy(ba.begin(), ba.end(), bw_csr);
+}
+
+graph::~graph() {
+    delete[] fw_beg_pos;
+    delete[] fw_csr;
+    delete[] bw_beg_pos;
+    delete[] bw_csr;
+}
+
+graph* graph::fromEdges(index_t V, const std::vector<std::pair<int, int>>& edges) {
+    auto* g = new graph();
+    const int64_t E = (int64_t)edges.size();
+    g->vert_count = V;
+    g->edge_count = (index_t)E;
+    g->fw_beg_pos = new index_t[V + 1]();
+    g->bw_beg_pos = new index_t[V + 1]();
+    g->fw_csr = new vertex_t[E > 0 ? E : 1];
+    g->bw_csr = new vertex_t[E > 0 ? E : 1];
+    for (auto& e : edges) {
+        g->fw_beg_pos[e.first + 1]++;
+        g->bw_beg_pos[e.second + 1]++;
+    }
+    for (int v = 0; v < V; ++v) {
+        g->fw_beg_pos[v + 1] += g->fw_beg_pos[v];
+        g->bw_beg_pos[v + 1] += g->bw_beg_pos[v];
+    }
+    std::vector<index_t> fp(g->fw_beg_pos, g->fw_beg_pos + V), bp(g->bw_beg_pos, g->bw_beg_pos + V);
+    for (auto& e : edges) {
+        g->fw_csr[fp[e.first]++] = e.second;
+        g->bw_csr[bp[e.second]++] = e.first;
+    }
+    return g;
+}
+
+GIR::GIR(graph* g) {
+    if (!g) throw Error(GIR_ERR_INVALID, "GIR(graph*): null graph");
+    std::unique_ptr<graph> own(g);
+    gir_dev_t* h = nullptr;
+    const int rc = gir_dev_create(g->fw_beg_pos, g->fw_csr, g->bw_beg_pos, g->bw_csr, g->vert_count, g->edge_count,
+                                  nullptr, &h);
+    if (rc != GIR_OK) throw Error(rc, std::string("gir_dev_create: ") + gir_dev_last_error(nullptr));
+    h_ = h;
+    V_ = g->vert_count;
+}
+
 GIR::GIR(GIR&& o) noexcept : h_(o.h_), V_(o.V_) { o.h_ = nullptr; }
 GIR& GIR::operator=(GIR&& o) noexcept {
     if (this != &o) {
@@ -95,6 +185,22 @@ void GIR::applyBatch(const std::vector<Update>& batch) {
         ins[i] = batch[i].insert ? 1 : 0;
     }
     check(gir_dev_apply_batch(h_, u.data(), v.data(), ins.data(), (int64_t)batch.size()), "applyBatch");
+}
+void GIR::ingestBatch(const std::vector<Update>& batch) {
+    std::vector<int32_t> u(batch.size()), v(batch.size());
+    std::vector<uint8_t> ins(batch.size());
+    for (size_t i = 0; i < batch.size(); ++i) {
+        u[i] = batch[i].u;
+        v[i] = batch[i].v;
+        ins[i] = batch[i].insert ? 1 : 0;
+    }
+    check(gir_dev_ingest_batch(h_, u.data(), v.data(), ins.data(), (int64_t)batch.size()), "ingestBatch");
+}
+void GIR::sync() { check(gir_dev_sync(h_), "sync"); }
+bool GIR::synced() const {
+    int s = 1;
+    check(gir_dev_synced(h_, &s), "synced");
+    return s != 0;
 }
 void GIR::insertEdge(int u, int v) { applyBatch({{u, v, true}}); }
 void GIR::deleteEdge(int u, int v) { applyBatch({{u, v, false}}); }
@@ -201,10 +307,77 @@ bool GIR::hasUndirectedEdge(int u, int v) const {
     return out != 0;
 }
 
-std::vector<int> GIR::bfs(int source) { return bfsMany({source}); }
-std::vector<uint64_t> GIR::sssp(int source, uint64_t delta) { return ssspMany({source}, delta); }
+QueryVec<int> GIR::bfs(int source) {
+    QueryVec<int> out((size_t)V_);
+    check(gir_dev_bfs(h_, &source, 1, out.data()), "bfs");
+    return out;
+}
+QueryVec<uint64_t> GIR::sssp(int source, uint64_t delta) {
+    QueryVec<uint64_t> out((size_t)V_);
+    check(gir_dev_sssp(h_, &source, 1, delta, GIR_WEIGHT_HASH, out.data()), "sssp");
+    return out;
+}
+QueryVec<double> GIR::bc(const std::vector<int>& sources) {
+    QueryVec<double> out((size_t)V_);
+    check(gir_dev_bc(h_, sources.data(), (int64_t)sources.size(), out.data()), "bc");
+    return out;
+}
 
 bool GIR::reachable(int u, int v) { return reachableMany({u}, {v})[0] != 0; }
+
+bool GIR::reachableNoIndex(int u, int v) {
+    if (u < 0 || v < 0 || u >= V_ || v >= V_) return false;
+    if (u == v) return true;
+    return bfs(u)[(size_t)v] >= 0;
+}
+
+bool GIR::biconnected(int u, int v) {
+    sync();
+    if (u == v) return true;
+    if (u < 0 || v < 0 || u >= V_ || v >= V_) return false;
+    const auto scc = labels(GIR_LABEL_SCC);
+    if (scc[u] != scc[v]) return false;
+    const auto blk = labels(GIR_LABEL_BLOCK);
+    int64_t nb = 0;
+    check(gir_dev_get_blocks(h_, nullptr, 0, &nb), "biconnected");
+    std::vector<int32_t> head((size_t)nb);
+    if (nb) check(gir_dev_get_blocks(h_, head.data(), nb, &nb), "biconnected");
+    // a vertex lies in its own block and in every block it heads
+    return blk[u] == blk[v] || head[blk[v]] == u || head[blk[u]] == v;
+}
+
+bool GIR::checkBlockForestInvariants(std::string* why) const {
+    auto fail = [&](const char* m) {
+        if (why) *why = m;
+        return false;
+    };
+    const auto scc = labels(GIR_LABEL_SCC);
+    const auto blk = labels(GIR_LABEL_BLOCK);
+    const auto cnt = labels(GIR_LABEL_BCNT);
+    int64_t nb = 0;
+    check(gir_dev_get_blocks(h_, nullptr, 0, &nb), "checkBlockForestInvariants");
+    std::vector<int32_t> head((size_t)nb);
+    if (nb) check(gir_dev_get_blocks(h_, head.data(), nb, &nb), "checkBlockForestInvariants");
+    std::vector<int> members((size_t)nb, 0), headed((size_t)V_, 0), bscc((size_t)nb, -1);
+    for (int v = 0; v < V_; ++v) {
+        if (blk[v] < 0 || blk[v] >= nb) return fail("a vertex without a valid block");
+        ++members[blk[v]];
+        if (bscc[blk[v]] == -1) bscc[blk[v]] = scc[v];
+        else if (bscc[blk[v]] != scc[v]) return fail("a block spans two SCCs");
+    }
+    for (int64_t b = 0; b < nb; ++b) {
+        if (members[b] == 0) return fail("a block without members");
+        if (head[b] >= 0) {
+            if (scc[head[b]] != bscc[b]) return fail("a block's head lies in another SCC");
+            ++headed[head[b]];
+        }
+    }
+    for (int v = 0; v < V_; ++v)
+        if (cnt[v] != 1 + headed[v]) return fail("a block count differs from 1 + the blocks the vertex heads");
+    for (int64_t b = 0; b < nb; ++b)
+        if (head[b] >= 0 && cnt[head[b]] < 2) return fail("a head that is not an articulation point");
+    return true;
+}
 
 std::vector<uint8_t> GIR::reachableMany(const std::vector<int>& u, const std::vector<int>& v) {
     if (u.size() != v.size()) throw Error(GIR_ERR_INVALID, "reachable: u and v differ in length");

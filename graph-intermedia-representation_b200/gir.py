@@ -173,6 +173,21 @@ class DeviceGraph:
         ins = np.ascontiguousarray(ins, np.uint8)
         self._ck(dev_lib().gir_dev_apply_batch(self._h, ptr(u), ptr(v), ptr(ins), len(u)), "apply_batch")
 
+    def ingest_batch(self, u, v, ins):
+        """Edge store only; the layers wait for sync() (gir_dev_ingest_batch)."""
+        u = np.ascontiguousarray(u, np.int32)
+        v = np.ascontiguousarray(v, np.int32)
+        ins = np.ascontiguousarray(ins, np.uint8)
+        self._ck(dev_lib().gir_dev_ingest_batch(self._h, ptr(u), ptr(v), ptr(ins), len(u)), "ingest_batch")
+
+    def sync(self):
+        self._ck(dev_lib().gir_dev_sync(self._h), "sync")
+
+    def synced(self):
+        out = ctypes.c_int()
+        self._ck(dev_lib().gir_dev_synced(self._h, ctypes.byref(out)), "synced")
+        return bool(out.value)
+
     def batch_stats(self):
         vals = [ctypes.c_int64() for _ in range(4)]
         self._ck(dev_lib().gir_dev_batch_stats(self._h, *[ctypes.byref(v) for v in vals]), "batch_stats")
@@ -371,14 +386,16 @@ class GIR:
         # gir.cpp:3134: the reference routes the undirected entry point through the directed one
         self._d.apply_batch([u], [v], [1 if insert else 0])
 
+    # deferred maintenance (gir.h:107-116): the edge store takes the batch now, the layers at sync()
     def ingestBatch(self, batch):
-        self.applyBatch(batch)
+        arr = np.asarray(list(batch), dtype=np.int64).reshape(-1, 3)
+        self._d.ingest_batch(arr[:, 0], arr[:, 1], arr[:, 2] != 0)
 
     def sync(self):
-        pass
+        self._d.sync()
 
     def synced(self):
-        return True
+        return self._d.synced()
 
     # per-vertex queries (gir.h:122-125)
     def vertexCount(self):
@@ -464,6 +481,67 @@ class GIR:
     def reachable(self, u, v):
         """gir.h:128-130 (gir_query.cpp:789-825); batches go through DeviceGraph.reachable."""
         return bool(self._d.reachable([u], [v])[0])
+
+    def reachableNoIndex(self, u, v):
+        """gir.h:138: the same answer without the index (a BFS from u over the edge store)."""
+        if not (0 <= u < self._V and 0 <= v < self._V):
+            return False
+        return u == v or bool(self._d.bfs([u])[0][v] >= 0)
+
+    # structure-based queries sync first (gir.h:131-135)
+    def sameScc(self, u, v):
+        self.sync()
+        lab = self._d.labels(native.LABEL_SCC)
+        return bool(lab[u] == lab[v])
+
+    def sameWcc(self, u, v):
+        self.sync()
+        lab = self._d.labels(native.LABEL_WCC)
+        return bool(lab[u] == lab[v])
+
+    def articulationPoint(self, v):
+        self.sync()
+        return self.isArticulationPoint(v)
+
+    def biconnected(self, u, v):
+        """u and v share a block of one SCC's undirected view (a vertex lies in its own block and
+        in every block it heads)."""
+        self.sync()
+        if u == v:
+            return True
+        scc = self._d.labels(native.LABEL_SCC)
+        if scc[u] != scc[v]:
+            return False
+        blk, head = self._d.blocks()
+        return bool(blk[u] == blk[v] or head[blk[v]] == u or head[blk[u]] == v)
+
+    def checkBlockForestInvariants(self):
+        """gir.h:153 (gir.cpp:4159-4211): the block-cut forest's structural rules -- every block
+        non-empty and inside one SCC with its head, heads are articulation points, block counts
+        equal 1 + the blocks a vertex heads."""
+        scc = self._d.labels(native.LABEL_SCC).astype(np.int64)
+        blk, head = self._d.blocks()
+        cnt = self._d.labels(native.LABEL_BCNT).astype(np.int64)
+        blk = blk.astype(np.int64)
+        head = head.astype(np.int64)
+        nb = len(head)
+        if len(blk) and (blk.min() < 0 or blk.max() >= nb):
+            return False
+        members = np.bincount(blk, minlength=nb)
+        if np.any(members == 0):
+            return False
+        lo = np.full(nb, np.iinfo(np.int64).max)
+        hi = np.full(nb, -1)
+        np.minimum.at(lo, blk, scc)
+        np.maximum.at(hi, blk, scc)
+        if np.any(lo != hi):
+            return False
+        hh = head >= 0
+        if np.any(scc[head[hh]] != lo[hh]):
+            return False
+        exp = np.ones(self._V, np.int64)
+        np.add.at(exp, head[hh], 1)
+        return bool(np.array_equal(cnt, exp) and np.all(cnt[head[hh]] >= 2))
 
     # gir.h:208-216: the reference's task-parallel formulations of the same queries (a wavefront
     # over the condensation DAG with block tasks inside SCCs) return what bfs / sssp return; on

@@ -36,6 +36,7 @@ DEV_SYMBOLS = (
     "gir_dev_sched_grad", "gir_dev_bfs_noalloc", "gir_dev_sched_trace", "gir_dev_sched_delta_choices",
     "gir_dev_batch_times", "gir_dev_batch_plan", "gir_dev_autotune", "gir_dev_reachable", "gir_dev_bc",
     "gir_dev_inc_track", "gir_dev_inc_update", "gir_dev_inc_dist", "gir_dev_single_stats",
+    "gir_dev_ingest_batch", "gir_dev_sync", "gir_dev_synced",
 )
 GEN_SYMBOLS = (
     "gir_gen_last_error", "gir_gen_free", "gir_gen_hash3", "gir_gen_rmat", "gir_gen_lattice", "gir_gen_csr",
@@ -91,6 +92,9 @@ def dev_lib():
             "gir_dev_sssp": [_P, _P, _I64, ctypes.c_uint64, ctypes.c_int, _P],
             "gir_dev_sssp_sets": [_P, _P, _P, _I64, ctypes.c_uint64, ctypes.c_int, _P],
             "gir_dev_apply_batch": [_P, _P, _P, _P, _I64],
+            "gir_dev_ingest_batch": [_P, _P, _P, _P, _I64],
+            "gir_dev_sync": [_P],
+            "gir_dev_synced": [_P, _P],
             "gir_dev_set_weight_rule": [_P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32],
             "gir_dev_batch_stats": [_P] + [ctypes.POINTER(_I64)] * 4,
             "gir_dev_set_schedule": [_P, ctypes.c_int],

@@ -11,20 +11,89 @@
 //    also has empty slots, for retired ids);
 //  - single-edge updates run as one-edge batches (same layers as the reference's
 //    Scope-Prune-Update path, gir.cpp:3043-3131);
+//  - bfsTwoLevel / bfsTaskParallel / ssspTwoLevel return the flat device queries' results (the
+//    reference's task-parallel formulations compute the same levels and distances);
+//  - checkBlockForestInvariants checks the representation's structural rules (every block
+//    non-empty and inside one SCC with its head, heads are articulation points, block counts
+//    match the heads) and does not re-derive biconnectivity;
 //  - malformed input throws gir_b200::Error with the GIR_ERR_* code, where the reference exits
 //    (graph.cpp:95-114, gir.cpp:122-126).
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
+#include <memory>
+#include <new>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <unordered_set>
+#include <utility>
 #include <vector>
 
 #include "gir_dev.h"
 
 namespace gir_b200 {
+
+// Query results (gir.h:25-37): a std::vector whose allocator leaves elements default-initialized
+// when the vector is sized, so a result row of V entries is not zeroed before the library fills
+// it. Compares equal with a std::vector of the same contents.
+template <class T>
+struct DefaultInitAllocator : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = DefaultInitAllocator<U>;
+    };
+    DefaultInitAllocator() = default;
+    template <class U>
+    DefaultInitAllocator(const DefaultInitAllocator<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using QueryVec = std::vector<T, DefaultInitAllocator<T>>;
+template <class T>
+bool operator==(const QueryVec<T>& a, const std::vector<T>& b) {
+    return a.size() == b.size() && std::equal(a.begin(), a.end(), b.begin());
+}
+template <class T>
+bool operator==(const std::vector<T>& a, const QueryVec<T>& b) { return b == a; }
+template <class T>
+bool operator!=(const QueryVec<T>& a, const std::vector<T>& b) { return !(a == b); }
+template <class T>
+bool operator!=(const std::vector<T>& a, const QueryVec<T>& b) { return !(b == a); }
+
+typedef int index_t;   // util.h:17-21
+typedef int vertex_t;
+
+// The reference's loader class (graph.h:11-57): the int32 four-array CSR in host memory, read from
+// the four .bin files or built from an edge list. GIR(graph*) takes ownership of it.
+class graph {
+public:
+    index_t* fw_beg_pos = nullptr;
+    vertex_t* fw_csr = nullptr;
+    index_t* bw_beg_pos = nullptr;
+    vertex_t* bw_csr = nullptr;
+    double* weight = nullptr;  // (unused, as in the reference)
+    index_t vert_count = 0;
+    index_t edge_count = 0;
+
+    graph() = default;
+    // graph.cpp:2-120: reads the four files; a missing, short or malformed file throws Error.
+    graph(const char* fw_beg_file, const char* fw_csr_file, const char* bw_beg_file, const char* bw_csr_file);
+    ~graph();
+    graph(const graph&) = delete;
+    graph& operator=(const graph&) = delete;
+    // graph.cpp:123-136: forward and backward CSR of an edge list (rows in edge order); caller owns.
+    static graph* fromEdges(index_t V, const std::vector<std::pair<int, int>>& edges);
+};
 
 class Error : public std::runtime_error {
 public:
@@ -62,6 +131,8 @@ public:
     GIR(int V, const std::vector<int>& fw_beg, const std::vector<int>& fw_adj, const std::vector<int>& bw_beg,
         const std::vector<int>& bw_adj, const std::vector<uint32_t>* weights = nullptr);
     static GIR fromEdges(int V, const std::vector<std::pair<int, int>>& edges);
+    // GIR(graph*) (gir.h:95): takes ownership of g (its arrays go to the GPU; g is deleted).
+    explicit GIR(graph* g);
     GIR(GIR&& o) noexcept;
     GIR& operator=(GIR&& o) noexcept;
     GIR(const GIR&) = delete;
@@ -77,9 +148,11 @@ public:
     void insertEdge(int u, int v);
     void deleteEdge(int u, int v);
     void applyBatch(const std::vector<Update>& batch);
-    void ingestBatch(const std::vector<Update>& batch) { applyBatch(batch); }
-    void sync() {}
-    bool synced() const { return true; }
+    // Deferred maintenance (gir.h:107-116): ingestBatch changes the edge store only; the layer
+    // getters describe the last sync until sync(); updates and structure-based queries sync first.
+    void ingestBatch(const std::vector<Update>& batch);
+    void sync();
+    bool synced() const;
     void updateEdgeDirected(int u, int v, bool insert);
     void updateEdgeUndirected(int u, int v, bool insert);  // routed as directed, as gir.cpp:3134 does
 
@@ -88,9 +161,12 @@ public:
     int wccOf(int v) const;
     long long sccRank(int s) const;
     bool isArticulationPoint(int v) const;
-    bool sameScc(int u, int v) const { return sccOf(u) == sccOf(v); }
-    bool sameWcc(int u, int v) const { return wccOf(u) == wccOf(v); }
-    bool articulationPoint(int v) const { return isArticulationPoint(v); }
+    // gir.h:131-138: structure-based queries sync first
+    bool sameScc(int u, int v) { sync(); return sccOf(u) == sccOf(v); }
+    bool sameWcc(int u, int v) { sync(); return wccOf(u) == wccOf(v); }
+    bool articulationPoint(int v) { sync(); return isArticulationPoint(v); }
+    // u and v share a block of one SCC's undirected view
+    bool biconnected(int u, int v);
     int vertexCount() const { return V_; }
 
     // materialized views (gir.h:142-153)
@@ -101,6 +177,9 @@ public:
     std::vector<std::vector<int>> getWCCs() const;
     std::vector<std::vector<int>> getBCTComponents(int scc_id) const;
     BlockCutTree* getBCT(int scc_id) const;  // caller owns
+    // gir.h:153 (gir.cpp:4159-4211): the block-cut forest's structural rules; *why gets the first
+    // broken rule.
+    bool checkBlockForestInvariants(std::string* why = nullptr) const;
 
     // edge store (gir.h:160-164)
     std::vector<int> getDirectedOutNeighbors(int v) const;
@@ -109,11 +188,18 @@ public:
     bool hasDirectedEdge(int u, int v) const;
     bool hasUndirectedEdge(int u, int v) const;
 
-    // queries (gir.h:204-216)
-    std::vector<int> bfs(int source);
-    std::vector<uint64_t> sssp(int source, uint64_t delta = 16);
+    // queries (gir.h:204-219)
+    QueryVec<int> bfs(int source);
+    QueryVec<int> bfsTwoLevel(int source) { return bfs(source); }
+    QueryVec<int> bfsTaskParallel(int source) { return bfs(source); }
+    QueryVec<uint64_t> sssp(int source, uint64_t delta = 16);
+    QueryVec<uint64_t> ssspTwoLevel(int source, uint64_t delta = 16) { return sssp(source, delta); }
+    // gir.h:219 (gir_query.cpp:728-778): Brandes betweenness summed over the sources
+    QueryVec<double> bc(const std::vector<int>& sources);
     // gir.h:128-130: u ~> v (needs buildSCC_DAG); reachableMany answers a batch of pairs.
     bool reachable(int u, int v);
+    // gir.h:138: the same answer without the index (a BFS from u on the edge store)
+    bool reachableNoIndex(int u, int v);
     std::vector<uint8_t> reachableMany(const std::vector<int>& u, const std::vector<int>& v);
     static uint32_t edgeWeight(int u, int v);
     // gir.h:220-232 (gir_query.cpp:867-996): incremental single-source BFS (weighted false) /

@@ -151,6 +151,18 @@ int gir_dev_sssp_sets(gir_dev_t* g, const int64_t* set_beg, const int32_t* set_s
  * lo, hi) set by gir_dev_set_weight_rule (default: the hash weight of GIR::edgeWeight). */
 int gir_dev_apply_batch(gir_dev_t* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n);
 
+/* Deferred maintenance: ingestBatch / sync / synced (gir.h:107-116, gir.cpp:3588-3632).
+ * gir_dev_ingest_batch applies a batch to the edge store only (the same batch semantics as
+ * apply_batch; incremental BFS / SSSP logs see it); the WCC / SCC / block layers keep describing
+ * the graph as of the last sync, so the label, DAG and block getters return that state. BFS, SSSP
+ * and betweenness read the edge store and see every ingested change. gir_dev_sync brings every
+ * built layer up to date with all batches ingested since the last sync, in one repair.
+ * gir_dev_apply_batch, gir_dev_build and gir_dev_reachable sync first, as the reference's updates
+ * and structure-based queries do. *synced = 1 when nothing is pending. */
+int gir_dev_ingest_batch(gir_dev_t* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n);
+int gir_dev_sync(gir_dev_t* g);
+int gir_dev_synced(gir_dev_t* g, int* synced);
+
 /* Wall time (ms) of the phases of the last apply_batch: [0] normalisation and the merges into the
  * edge store, [1] WCC, [2] SCC + DAG + ranks, [3] blocks. */
 int gir_dev_batch_times(gir_dev_t* g, double* ms4);

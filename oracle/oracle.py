@@ -92,6 +92,10 @@ def ref():
         R.ref_bc.restype = None
         R.ref_ingest_batch.argtypes = [_P, _P, _P, _P, _I64]
         R.ref_ingest_batch.restype = None
+        R.ref_sync.argtypes = [_P]
+        R.ref_sync.restype = None
+        R.ref_synced.argtypes = [_P]
+        R.ref_synced.restype = ctypes.c_int
         R.ref_inc_track.argtypes = [_P, ctypes.c_int32, ctypes.c_int]
         R.ref_inc_track.restype = None
         R.ref_inc_update.argtypes = [_P, ctypes.c_int]
@@ -461,6 +465,13 @@ class RefGIR:
         v = np.ascontiguousarray(v, np.int32)
         ins = np.ascontiguousarray(ins, np.uint8)
         ref().ref_ingest_batch(self.h, ptr(u), ptr(v), ptr(ins), len(u))
+
+    def sync(self):
+        """GIR::sync: the layers catch up with the ingested batches."""
+        ref().ref_sync(self.h)
+
+    def synced(self):
+        return bool(ref().ref_synced(self.h))
 
     def update_edge(self, u, v, insert, undirected=False):
         ref().ref_update_edge(self.h, u, v, int(insert), int(undirected))

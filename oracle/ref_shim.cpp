@@ -99,6 +99,10 @@ void ref_ingest_batch(void* h, const int32_t* u, const int32_t* v, const uint8_t
     static_cast<GIR*>(h)->ingestBatch(b);
 }
 
+// GIR::sync / synced (gir.h:115-116).
+void ref_sync(void* h) { static_cast<GIR*>(h)->sync(); }
+int ref_synced(void* h) { return static_cast<GIR*>(h)->synced() ? 1 : 0; }
+
 void ref_update_edge(void* h, int32_t u, int32_t v, int insert, int undirected) {
     GIR* g = static_cast<GIR*>(h);
     if (undirected) g->updateEdgeUndirected(u, v, insert != 0);

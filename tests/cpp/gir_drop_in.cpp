@@ -4,6 +4,8 @@
 // tests/test_gpu_cpp_class.py compiles it against include/gir_b200.hpp and libgir_b200.so.
 #include <cstdio>
 #include <memory>
+#include <string>
+#include <vector>
 
 #include "gir_b200.hpp"
 
@@ -65,6 +67,40 @@ int main(int argc, char** argv) {
             inc_ok = inc_ok && g.incDist(false, v) == (lv2[v] < 0 ? UINT64_MAX : (uint64_t)lv2[v]) &&
                      g.incDist(true, v) == d2[v];
         std::printf("inc_matches_scratch %d\n", (int)inc_ok);
+        // query results are QueryVec (gir.h:32-37) and compare with plain vectors
+        gir_b200::QueryVec<int> q = g.bfs(0);
+        std::vector<int> plain(q.begin(), q.end());
+        std::printf("queryvec %d\n", (int)(q == plain && !(q != plain) && g.bfsTwoLevel(0) == plain));
+        bool nidx = true;
+        for (int v = 0; v < g.vertexCount(); ++v) nidx = nidx && g.reachableNoIndex(0, v) == g.reachable(0, v);
+        std::printf("reach_noindex %d\n", (int)nidx);
+        std::string why;
+        std::printf("forest_ok %d\n", (int)g.checkBlockForestInvariants(&why));
+        std::printf("bicon_self %d\n", (int)g.biconnected(5, 5));
+        const auto bcv = g.bc({0, 1, 2});
+        bool bc_ok = (int)bcv.size() == g.vertexCount();
+        for (double x : bcv) bc_ok = bc_ok && x >= 0;
+        std::printf("bc_ok %d\n", (int)bc_ok);
+        // deferred maintenance (gir.h:107-116): ingestBatch changes the edge store now, the layers
+        // at sync(); BFS sees the change at once
+        const int w_before = (int)g.getWCCs().size();
+        const int joins = g.wccOf(3) != g.wccOf(12);
+        g.ingestBatch({{3, 12, true}});
+        const int pending = !g.synced();
+        const int w_pending = (int)g.getWCCs().size();
+        const int bfs_sees = g.bfs(3)[12] == 1;
+        g.sync();
+        std::printf("ingest %d %d %d %d\n", pending, (int)(w_pending == w_before), bfs_sees,
+                    (int)((int)g.getWCCs().size() == w_before - joins && g.synced()));
+        // GIR(graph*): the reference's loader type, from graph::fromEdges and from the four files
+        GIR h(gir_b200::graph::fromEdges(4, {{0, 1}, {1, 2}, {2, 0}, {2, 3}}));
+        h.buildWCC();
+        h.buildSCC_DAG();
+        h.buildBCT();
+        const std::string dir = argv[1];
+        GIR f(new gir_b200::graph((dir + "fw_begin.bin").c_str(), (dir + "fw_adjacent.bin").c_str(),
+                                  (dir + "bw_begin.bin").c_str(), (dir + "bw_adjacent.bin").c_str()));
+        std::printf("from_graph %d %d %d\n", h.vertexCount(), count_nonempty(h.getSCCs()), f.vertexCount());
         try {
             GIR bad("/nonexistent/dir/", "/nonexistent/dir/");
             std::printf("error_missing 0\n");

@@ -40,3 +40,7 @@ def test_cpp_caller_on_example_graph(golden, tmp_path):
     assert kv["reach_matches_bfs"] == ["1"]
     assert kv["inc_matches_scratch"] == ["1"]
     assert kv["error_missing"] == ["1"]
+    assert kv["queryvec"] == ["1"] and kv["reach_noindex"] == ["1"]
+    assert kv["forest_ok"] == ["1"] and kv["bicon_self"] == ["1"] and kv["bc_ok"] == ["1"]
+    assert kv["ingest"] == ["1", "1", "1", "1"]  # pending, getters unchanged, BFS sees it, synced
+    assert kv["from_graph"] == ["4", "2", "18"]

@@ -109,6 +109,18 @@ def test_gir_class_surface(pkg, golden):
     assert G.hasDirectedEdge(2, 9) and not G.hasDirectedEdge(9, 2) and G.hasUndirectedEdge(9, 2)
     assert G.bfs(0)[9] == 3  # 0 -> 1 -> 2 -> 9
     assert G.sssp(0)[0] == 0 and G.sssp(0)[1] == G.edgeWeight(0, 1)
+    # structure queries (gir.h:131-138, 153)
+    assert G.sameScc(0, 1) and not G.sameScc(0, 9) and G.sameWcc(0, 9)
+    assert G.biconnected(0, 1) and not G.biconnected(0, 9) and G.biconnected(4, 4)
+    assert all(G.reachableNoIndex(0, v) == G.reachable(0, v) for v in range(18))
+    assert G.checkBlockForestInvariants()
+    assert not any(G.articulationPoint(v) for v in (0, 1, 2))
+    # deferred maintenance: the layers wait for sync (gir.h:107-116)
+    wccs = len(G.getWCCs())
+    G.ingestBatch([(3, 12, True)])
+    assert not G.synced() and len(G.getWCCs()) == wccs and G.bfs(3)[12] == 1
+    G.sync()
+    assert G.synced() and len(G.getWCCs()) == wccs - 1
 
 
 @pytest.fixture(scope="module")
@@ -330,4 +342,58 @@ def test_reachable_matches_reference(pkg, orc, s16):
         gg = pkg.graphs.Graph(g.V, cb.astype(np.int32), ca, None, None)
         bu, bv, bi = pkg.graphs.updates(gg, 3000, 3000, 41)
         d.apply_batch(bu, bv, bi)
+    d.close()
+
+
+def test_ingest_and_sync_match_reference(pkg, orc, s16):
+    """GIR::ingestBatch / sync (gir.h:107-116): ingested batches change the edge store at once (BFS
+    sees them) while the layer getters keep describing the last sync, like the reference's own
+    ingestBatch; sync() repairs every layer for all of them at once; applyBatch and reachability
+    sync first."""
+    if not orc.ref_available():
+        pytest.skip("the reference library oracle/_ref/libgirref.so is not built")
+    g, fb, fa = s16
+    ref = orc.RefGIR(g.V, g.fw_beg, g.fw_adj, g.bw_beg, g.bw_adj)
+    ref.build(7)
+    d = pkg.DeviceGraph.from_graph(g)
+    d.build(pkg.native.LAYER_ALL)
+    before = _layers(pkg, orc, d)
+    assert d.synced()
+    src = pkg.graphs.sources(g.V, 3, 5)
+    for k, (ni, nd) in enumerate(((300, 300), (0, 2000), (1500, 0))):
+        cb, ca = d.csr(0)
+        u, v, ins = pkg.graphs.updates(pkg.graphs.Graph(g.V, cb.astype(np.int32), ca, None, None), ni, nd, 900 + k)
+        d.ingest_batch(u, v, ins)
+        ref.ingest_batch(u, v, ins)
+        assert not d.synced() and not ref.synced()
+        now = _layers(pkg, orc, d)
+        for a, b, what in zip(before, now, ("wcc", "scc", "dag", "blocks", "ap")):
+            np.testing.assert_array_equal(a, b, err_msg=f"ingest {k}: {what} changed before sync")
+        np.testing.assert_array_equal(now[0], ref.wcc(), err_msg=f"ingest {k}: WCC vs the reference before sync")
+        np.testing.assert_array_equal(now[1], ref.scc(), err_msg=f"ingest {k}: SCC vs the reference before sync")
+        lv = d.bfs(src)
+        for i, s in enumerate(src):
+            np.testing.assert_array_equal(lv[i], ref.bfs(int(s)), err_msg=f"ingest {k}: BFS sees the store")
+    d.sync()
+    ref.sync()
+    assert d.synced() and ref.synced()
+    cb, ca = d.csr(0)
+    _oracle_match(pkg, orc, d, g.V, cb, ca, "after sync")
+    wcc, scc, dag, blocks, ap = _layers(pkg, orc, d)
+    np.testing.assert_array_equal(scc, ref.scc())
+    np.testing.assert_array_equal(wcc, ref.wcc())
+    np.testing.assert_array_equal(dag, ref.dag())
+    np.testing.assert_array_equal(blocks, ref.blocks())
+    # reachability and applyBatch sync pending batches first
+    cb, ca = d.csr(0)
+    u, v, ins = pkg.graphs.updates(pkg.graphs.Graph(g.V, cb.astype(np.int32), ca, None, None), 200, 200, 950)
+    d.ingest_batch(u, v, ins)
+    d.reachable([0], [1])
+    assert d.synced()
+    d.ingest_batch(v, u, ins)
+    d.apply_batch(u[:10], v[:10], 1 - ins[:10])
+    assert d.synced()
+    cb, ca = d.csr(0)
+    _oracle_match(pkg, orc, d, g.V, cb, ca, "after apply_batch on pending batches")
+    ref.close()
     d.close()

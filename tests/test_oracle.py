@@ -152,3 +152,28 @@ def test_reference_incremental_matches_oracle(orc, pkg):
         np.testing.assert_array_equal(r.inc_dist(False), np.where(lv < 0, none, lv.astype(np.uint64)))
         np.testing.assert_array_equal(r.inc_dist(True), orc.sssp(g.V, beg, adj, [src]))
     r.close()
+
+
+def test_reference_ingest_defers_layers_until_sync(orc, pkg):
+    """Pins the checker of the deferred-maintenance test: the reference's own ingestBatch leaves its
+    layer getters at the last sync, and sync() brings them to the oracle's answer for the new
+    graph."""
+    if not orc.ref_available():
+        import pytest
+        pytest.skip("the reference library is not built")
+    g = pkg.graphs.rmat(11, seed=4, weights=None)
+    fb, fa = orc.normalize(g.V, g.fw_beg, g.fw_adj)
+    r = orc.RefGIR(g.V, g.fw_beg, g.fw_adj, g.bw_beg, g.bw_adj)
+    r.build(7)
+    scc0 = r.scc()
+    u, v, ins = pkg.graphs.updates(g, 300, 600, 8)
+    r.ingest_batch(u, v, ins)
+    assert not r.synced()
+    np.testing.assert_array_equal(r.scc(), scc0)
+    r.sync()
+    fb2, fa2, _, _ = orc.apply_batch(g.V, fb, fa, u, v, ins)
+    L2 = orc.Layers(g.V, fb2, fa2)
+    np.testing.assert_array_equal(r.scc(), L2.scc)
+    np.testing.assert_array_equal(r.wcc(), L2.wcc)
+    np.testing.assert_array_equal(r.blocks(), L2.blocks)
+    r.close()

@@ -398,6 +398,100 @@ int rebuild_layers(gir_dev* g, const RepairPlan& plan) {
     return GIR_OK;
 }
 
+// The repair plan of an applied batch from its flags (judged with the labels from before it),
+// its symmetric-pair changes (nsi pairs made present, keys sym_ins on the device; nsd removed) and
+// its directed changes; a batch of exactly one change (one_key) asks the exact searches of
+// single.cu first. Then every built layer is brought up to date.
+static int plan_and_repair(gir_dev* g, const unsigned long long* fl, int64_t nsi, int64_t nsd, const uint64_t* sym_ins,
+                           int64_t n_ins, int64_t n_del, uint64_t one_key) {
+    RepairPlan plan;
+    plan.wcc = nsd > 0 ? REBUILD : (nsi > 0 ? PATCH : KEEP);
+    plan.pairs_in = sym_ins;
+    plan.n_pairs_in = nsi;
+    plan.scc = (fl[F_SCC_SPLIT] || fl[F_SCC_CYCLE]) ? REBUILD : (fl[F_DAG] ? PATCH : KEEP);
+    plan.bct = fl[F_BCT] ? REBUILD : KEEP;
+    if (n_ins + n_del == 1) {
+        // one change: exact searches settle what the flags leave open (single.cu)
+        SingleChecks want;
+        want.wcc = g->wcc_built && nsd > 0;
+        want.split = g->scc_built && fl[F_SCC_SPLIT];
+        want.cycle = g->scc_built && fl[F_SCC_CYCLE];
+        want.twopath = g->bct_built && fl[F_BCT] && n_del == 1 && nsd > 0;
+        int32_t res[4];
+        GIR_TRY(single_op_checks(g, (int32_t)(one_key >> 32), (int32_t)(uint32_t)one_key, want, res));
+        if (want.wcc || want.split || want.cycle || want.twopath) ++g->single_checked;
+        if (want.wcc && res[0] == 1) { plan.wcc = KEEP; ++g->single_kept; }
+        if (want.wcc && res[0] == 4) {  // the component split, labels already updated in place
+            plan.wcc = KEEP;
+            ++g->n_wcc;
+            ++g->single_kept;
+        }
+        if (want.split && res[1] == 1) { plan.scc = fl[F_DAG] ? PATCH : KEEP; ++g->single_kept; }
+        if (want.cycle && res[2] == 2) { plan.scc = PATCH; ++g->single_kept; }
+        if (want.twopath && res[3] == 1 && plan.scc != REBUILD) { plan.bct = KEEP; ++g->single_kept; }
+        if (plan.scc == PATCH && !fl[F_SCC_CYCLE]) {  // a cross-SCC change along the rank order
+            plan.one_edge = true;
+            plan.u = (int32_t)(one_key >> 32);
+            plan.v = (int32_t)(uint32_t)one_key;
+            plan.insert = n_ins == 1;
+        }
+    }
+    g->b_plan[0] = plan.wcc;
+    g->b_plan[1] = plan.scc;
+    g->b_plan[2] = plan.scc == REBUILD ? REBUILD : plan.bct;
+    GIR_TRY(rebuild_layers(g, plan));
+    return GIR_OK;
+}
+
+// The single-edge latency path for a one-op batch of host arrays: the change is applied to the
+// three slack rows in place by one CTA, which also judges the layer flags (store_single_edit),
+// so the batch normalisation, sorts and merges are skipped. *handled = 0 sends the op through
+// the batch path (device arrays, or a row without room for an insert).
+static int single_fast(gir_dev* g, const int32_t* u, const int32_t* v, const uint8_t* ins, int* handled) {
+    *handled = 0;
+    if (is_device_ptr(u) || is_device_ptr(v) || is_device_ptr(ins)) return GIR_OK;
+    const int32_t a = *u, b = *v;
+    const int insert = *ins != 0;
+    const double t_start = now_ms();
+    if (a == b || a < 0 || b < 0 || a >= g->V || b >= g->V) {  // dropped, as normalizeBatch does
+        g->b_invalid = 1;
+        *handled = 1;
+        return GIR_OK;
+    }
+    unsigned long long* dw = nullptr;
+    GIR_TRY(ensure_n(g, g->work[7], 8, &dw));
+    uint64_t* keys = reinterpret_cast<uint64_t*>(dw + 4);
+    GIR_TRY(store_single_edit(g, a, b, insert, dw, keys));
+    void* hp = nullptr;
+    GIR_TRY(pinned(g, 256, &hp));
+    unsigned long long* hw = static_cast<unsigned long long*>(hp);
+    GIR_CUDA(g, cudaMemcpyAsync(hw, dw, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, g->stream));
+    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    const unsigned long long st = hw[0], symc = hw[1], bits = hw[2];
+    if (st == 2) return GIR_OK;
+    *handled = 1;
+    if (st == 0) {
+        g->b_noop = 1;
+        return GIR_OK;
+    }
+    const int64_t d = insert ? 1 : -1;
+    g->fw.E += d;
+    g->bw.E += d;
+    if (symc) g->sym.E += 2 * d;
+    g->b_ins = insert;
+    g->b_del = !insert;
+    GIR_TRY(inc_log(g, keys, insert, keys, !insert));
+    GIR_TRY(invalidate_after_update(g));
+    g->b_ms[0] = now_ms() - t_start;
+    unsigned long long fl[F_N] = {};
+    fl[F_SCC_SPLIT] = bits & 1;
+    fl[F_SCC_CYCLE] = (bits >> 1) & 1;
+    fl[F_DAG] = (bits >> 2) & 1;
+    fl[F_BCT] = (bits >> 3) & 1;
+    const uint64_t one_key = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
+    return plan_and_repair(g, fl, symc == 1 ? 2 : 0, symc == 2 ? 2 : 0, keys + 1, insert, !insert, one_key);
+}
+
 // sync (gir.cpp:3602-3632): the layers catch up with every batch ingested since the last sync,
 // in one repair whose plan joins what each of those batches could change.
 int sync_impl(gir_dev* g) {
@@ -431,6 +525,11 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
     for (int& x : g->b_plan) x = 0;  // (a batch without effective ops keeps every layer)
     const double t_start = now_ms();
     if (n <= 0) return GIR_OK;
+    if (n == 1 && !deferred) {
+        int handled = 0;
+        GIR_TRY(single_fast(g, u, v, ins, &handled));
+        if (handled) return GIR_OK;
+    }
     trace_mark(g, "batch: start");
     const void *du, *dv, *dins;
     DevBuf su, sv, si;
@@ -582,43 +681,7 @@ int apply_batch_impl(gir_dev* g, const int32_t* u, const int32_t* v, const uint8
         }
         return GIR_OK;
     }
-    RepairPlan plan;
-    plan.wcc = nsd > 0 ? REBUILD : (nsi > 0 ? PATCH : KEEP);
-    plan.pairs_in = sym_ins;
-    plan.n_pairs_in = nsi;
-    plan.scc = (fl[F_SCC_SPLIT] || fl[F_SCC_CYCLE]) ? REBUILD : (fl[F_DAG] ? PATCH : KEEP);
-    plan.bct = fl[F_BCT] ? REBUILD : KEEP;
-    if (n_ins + n_del == 1) {
-        // one change: exact searches settle what the flags leave open (single.cu)
-        SingleChecks want;
-        want.wcc = g->wcc_built && nsd > 0;
-        want.split = g->scc_built && fl[F_SCC_SPLIT];
-        want.cycle = g->scc_built && fl[F_SCC_CYCLE];
-        want.twopath = g->bct_built && fl[F_BCT] && n_del == 1 && nsd > 0;
-        int32_t res[4];
-        GIR_TRY(single_op_checks(g, (int32_t)(one_key >> 32), (int32_t)(uint32_t)one_key, want, res));
-        if (want.wcc || want.split || want.cycle || want.twopath) ++g->single_checked;
-        if (want.wcc && res[0] == 1) { plan.wcc = KEEP; ++g->single_kept; }
-        if (want.wcc && res[0] == 4) {  // the component split, labels already updated in place
-            plan.wcc = KEEP;
-            ++g->n_wcc;
-            ++g->single_kept;
-        }
-        if (want.split && res[1] == 1) { plan.scc = fl[F_DAG] ? PATCH : KEEP; ++g->single_kept; }
-        if (want.cycle && res[2] == 2) { plan.scc = PATCH; ++g->single_kept; }
-        if (want.twopath && res[3] == 1 && plan.scc != REBUILD) { plan.bct = KEEP; ++g->single_kept; }
-        if (plan.scc == PATCH && !fl[F_SCC_CYCLE]) {  // a cross-SCC change along the rank order
-            plan.one_edge = true;
-            plan.u = (int32_t)(one_key >> 32);
-            plan.v = (int32_t)(uint32_t)one_key;
-            plan.insert = n_ins == 1;
-        }
-    }
-    g->b_plan[0] = plan.wcc;
-    g->b_plan[1] = plan.scc;
-    g->b_plan[2] = plan.scc == REBUILD ? REBUILD : plan.bct;
-    GIR_TRY(rebuild_layers(g, plan));
-    return GIR_OK;
+    return plan_and_repair(g, fl, nsi, nsd, sym_ins, n_ins, n_del, one_key);
 }
 
 int read_file_ints(const std::string& path, std::vector<int32_t>& out, int64_t n, gir_dev* g) {

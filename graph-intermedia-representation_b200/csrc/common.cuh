@@ -269,6 +269,11 @@ int store_has_edges(gir_dev* g, const DevCSR& c, const int32_t* u, const int32_t
 int store_apply_ops(gir_dev* g, DevCSR& c, const uint64_t* ins, int64_t n_ins, const uint64_t* del, int64_t n_del,
                     bool weights);
 int store_build_bins(gir_dev* g);
+// One change u -> v applied in place to the fw / bw / sym rows when they have room (store.cu):
+// out[0] 0 no-op, 1 applied, 2 no room (nothing changed); out[1] 1 / 2 when the undirected pair
+// appeared / disappeared; out[2] layer flags (bit 0 SCC split possible, 1 cycle closed against
+// the ranks, 2 a cross edge changed, 3 blocks may change); keys[0] the edge, keys[1..2] the pair.
+int store_single_edit(gir_dev* g, int32_t u, int32_t v, int insert, unsigned long long* out, uint64_t* keys);
 
 // ---- CUB wrappers (prims.cu) ----
 int sort_keys_u64(gir_dev* g, uint64_t* keys, uint64_t* tmp, int64_t n, int end_bit);

@@ -33,6 +33,21 @@ __device__ __forceinline__ int64_t row_of(const int64_t* cb, int64_t V, int64_t 
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
+// Stored weight of a newly inserted edge u -> x: the hash weight of GIR::edgeWeight when
+// wlo > whi, else w(u,v) = lo + hash3(seed,u,v) mod span, the generator's rule (csrc/gen.cpp).
+__device__ __forceinline__ uint32_t new_edge_weight(int32_t r, int32_t x, uint64_t wseed, uint32_t wlo, uint32_t whi) {
+    if (wlo > whi) return hash_weight(r, x);
+    uint64_t z = wseed ^ 0x5851f42d4c957f2dULL;
+    auto mix = [](uint64_t s) {
+        s += 0x9e3779b97f4a7c15ULL;
+        s = (s ^ (s >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        s = (s ^ (s >> 27)) * 0x94d049bb133111ebULL;
+        return s ^ (s >> 31);
+    };
+    const uint64_t h = mix(mix(z) ^ mix((uint64_t)(uint32_t)r * 0x2545f4914f6cdd1dULL + (uint64_t)(uint32_t)x));
+    return wlo + (uint32_t)(h % ((uint64_t)whi - wlo + 1));
+}
+
 // Head and tail positions of every row's run in a sorted key array.
 __global__ void k_row_runs(const uint64_t* keys, int64_t n, int64_t* first, int64_t* end) {
     GRID_STRIDE(i, n) {
@@ -167,24 +182,7 @@ __global__ void k_merge_rows(const uint64_t* ins, const uint64_t* del, const int
             const int64_t slot = q + po - (pd - db);
             if (slot < 0 || slot >= newdeg[k]) { atomicExch(bad, 1); continue; }
             tmp[toff[k] + slot] = x;
-            if (weights) {
-                uint32_t wv;
-                if (wlo > whi) {
-                    wv = hash_weight((int32_t)r, x);
-                } else {
-                    // w(u,v) = lo + hash3(seed,u,v) mod span: the generator's rule (csrc/gen.cpp)
-                    uint64_t z = wseed ^ 0x5851f42d4c957f2dULL;
-                    auto mix = [](uint64_t s) {
-                        s += 0x9e3779b97f4a7c15ULL;
-                        s = (s ^ (s >> 30)) * 0xbf58476d1ce4e5b9ULL;
-                        s = (s ^ (s >> 27)) * 0x94d049bb133111ebULL;
-                        return s ^ (s >> 31);
-                    };
-                    const uint64_t h = mix(mix(z) ^ mix((uint64_t)r * 0x2545f4914f6cdd1dULL + (uint64_t)(uint32_t)x));
-                    wv = wlo + (uint32_t)(h % ((uint64_t)whi - wlo + 1));
-                }
-                tmpw[toff[k] + slot] = wv;
-            }
+            if (weights) tmpw[toff[k] + slot] = new_edge_weight((int32_t)r, x, wseed, wlo, whi);
         }
     }
 }
@@ -267,7 +265,152 @@ __global__ void k_bin_flags(int64_t V, const int32_t* deg, int32_t small, int32_
     }
 }
 
+// ---- one edge, edited in place (the single-edge latency path) -------------------------------
+// Block-cooperative shifts of one row's entries (and weights): all reads of a chunk happen before
+// its writes, and chunks move away from the gap, so nothing is overwritten before it is read.
+__device__ void row_insert_at(int32_t* adj, uint32_t* w, int64_t p, int64_t end, int32_t x, uint32_t wx) {
+    for (int64_t hi = end; hi > p; hi -= blockDim.x) {
+        const int64_t lo = hi - (int64_t)blockDim.x > p ? hi - (int64_t)blockDim.x : p;
+        const int64_t i = lo + threadIdx.x;
+        const bool act = i < hi;
+        int32_t a = 0;
+        uint32_t b = 0;
+        if (act) { a = adj[i]; if (w) b = w[i]; }
+        __syncthreads();
+        if (act) { adj[i + 1] = a; if (w) w[i + 1] = b; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { adj[p] = x; if (w) w[p] = wx; }
+    __syncthreads();
+}
+
+__device__ void row_erase_at(int32_t* adj, uint32_t* w, int64_t p, int64_t end) {
+    for (int64_t lo = p + 1; lo < end; lo += blockDim.x) {
+        const int64_t i = lo + threadIdx.x;
+        const bool act = i < end;
+        int32_t a = 0;
+        uint32_t b = 0;
+        if (act) { a = adj[i]; if (w) b = w[i]; }
+        __syncthreads();
+        if (act) { adj[i - 1] = a; if (w) w[i - 1] = b; }
+        __syncthreads();
+    }
+}
+
+struct MutCSR {
+    const int64_t* beg;
+    int32_t* deg;
+    int32_t* adj;
+    uint32_t* w;
+};
+
+// One directed change u -> v on the three slack CSRs, in one CTA. out[0]: 0 no-op (the edge is
+// already present / absent), 1 applied, 2 a row lacks room (nothing changed: the batch merge
+// runs instead). out[1]: 1 when the undirected pair {u, v} appeared, 2 when it disappeared.
+// out[2]: layer flags judged with the current labels, as the batch classification does (bit 0
+// an edge inside an SCC deleted, bit 1 an inserted cross edge against the rank order, bit 2 a
+// cross edge changed, bit 3 the blocks may change). keys: u << 32 | v, then the two orientations
+// of the pair.
+__global__ void __launch_bounds__(1024) k_single_edit(MutCSR fw, MutCSR bw, MutCSR sym, int32_t u, int32_t v, int insert,
+                                                      int weights, uint64_t wseed, uint32_t wlo, uint32_t whi,
+                                                      const int32_t* scc, const int32_t* rank, const int32_t* blk,
+                                                      const int32_t* head, unsigned long long* out, uint64_t* keys) {
+    __shared__ int64_t s_pos[4];
+    __shared__ int s_st, s_sym;
+    if (threadIdx.x == 0) {
+        const int64_t fb = fw.beg[u], fd = fw.deg[u];
+        const int64_t pf = lower_bound_dev(fw.adj, fb, fb + fd, v);
+        const bool has_uv = pf < fb + fd && fw.adj[pf] == v;
+        const int64_t rb = fw.beg[v], rd = fw.deg[v];
+        const int64_t pr = lower_bound_dev(fw.adj, rb, rb + rd, u);
+        const bool has_vu = pr < rb + rd && fw.adj[pr] == u;
+        const int64_t bb = bw.beg[v], bd = bw.deg[v];
+        const int64_t pb = lower_bound_dev(bw.adj, bb, bb + bd, u);
+        const int64_t su = sym.beg[u], sdu = sym.deg[u], sv = sym.beg[v], sdv = sym.deg[v];
+        const int64_t psu = lower_bound_dev(sym.adj, su, su + sdu, v);
+        const int64_t psv = lower_bound_dev(sym.adj, sv, sv + sdv, u);
+        int st = 1, symc = 0;
+        if ((insert != 0) == has_uv) {
+            st = 0;
+        } else if (insert) {
+            symc = has_vu ? 0 : 1;
+            const bool room = fb + fd + 1 <= fw.beg[u + 1] && bb + bd + 1 <= bw.beg[v + 1] &&
+                              (!symc || (su + sdu + 1 <= sym.beg[u + 1] && sv + sdv + 1 <= sym.beg[v + 1]));
+            if (!room) st = 2;
+        } else {
+            symc = has_vu ? 0 : 2;
+        }
+        unsigned long long fl = 0;
+        if (st == 1 && scc) {
+            const bool same = scc[u] == scc[v];
+            if (!insert && same) fl |= 1;
+            if (!same) fl |= 4;
+            if (insert && !same && rank[u] >= rank[v]) fl |= 2;
+            if (symc && same && blk) {
+                if (symc == 2) fl |= 8;
+                else {
+                    const int32_t bu = blk[u], bv = blk[v];
+                    if (!(bu == bv || head[bv] == u || head[bu] == v)) fl |= 8;
+                }
+            }
+        }
+        s_pos[0] = pf; s_pos[1] = pb; s_pos[2] = psu; s_pos[3] = psv;
+        s_st = st;
+        s_sym = symc;
+        out[0] = (unsigned long long)st;
+        out[1] = (unsigned long long)symc;
+        out[2] = fl;
+        keys[0] = ((uint64_t)(uint32_t)u << 32) | (uint32_t)v;
+        keys[1] = keys[0];
+        keys[2] = ((uint64_t)(uint32_t)v << 32) | (uint32_t)u;
+    }
+    __syncthreads();
+    if (s_st != 1) return;
+    const int64_t fend = fw.beg[u] + fw.deg[u], bend = bw.beg[v] + bw.deg[v];
+    const int64_t suend = sym.beg[u] + sym.deg[u], svend = sym.beg[v] + sym.deg[v];
+    if (insert) {
+        row_insert_at(fw.adj, weights ? fw.w : nullptr, s_pos[0], fend, v,
+                      weights ? new_edge_weight(u, v, wseed, wlo, whi) : 0u);
+        row_insert_at(bw.adj, nullptr, s_pos[1], bend, u, 0u);
+        if (s_sym == 1) {
+            row_insert_at(sym.adj, nullptr, s_pos[2], suend, v, 0u);
+            row_insert_at(sym.adj, nullptr, s_pos[3], svend, u, 0u);
+        }
+    } else {
+        row_erase_at(fw.adj, weights ? fw.w : nullptr, s_pos[0], fend);
+        row_erase_at(bw.adj, nullptr, s_pos[1], bend);
+        if (s_sym == 2) {
+            row_erase_at(sym.adj, nullptr, s_pos[2], suend);
+            row_erase_at(sym.adj, nullptr, s_pos[3], svend);
+        }
+    }
+    if (threadIdx.x == 0) {
+        const int d = insert ? 1 : -1;
+        fw.deg[u] += d;
+        bw.deg[v] += d;
+        if (s_sym) {
+            sym.deg[u] += d;
+            sym.deg[v] += d;
+        }
+    }
+}
+
 }  // namespace
+
+// The single-edge latency path: u -> v inserted (insert != 0) or deleted in place (see
+// k_single_edit); the result words and keys are device arrays (3 and 3 entries) the caller reads.
+int store_single_edit(gir_dev* g, int32_t u, int32_t v, int insert, unsigned long long* out, uint64_t* keys) {
+    auto mut = [](DevCSR& c) { return MutCSR{c.beg, c.deg, c.adj, c.w}; };
+    const int32_t* scc = g->scc_built ? static_cast<const int32_t*>(g->scc.p) : nullptr;
+    const int32_t* rank = g->scc_built ? static_cast<const int32_t*>(g->scc_rank.p) : nullptr;
+    const int32_t* blk = g->bct_built ? static_cast<const int32_t*>(g->blk_label.p) : nullptr;
+    const int32_t* head = g->bct_built ? static_cast<const int32_t*>(g->blk_head.p) : nullptr;
+    k_single_edit<<<1, 1024, 0, g->stream>>>(mut(g->fw), mut(g->bw), mut(g->sym), u, v, insert,
+                                             g->has_weights && g->fw.w ? 1 : 0, g->wrule_seed, g->wrule_lo, g->wrule_hi,
+                                             scc, rank, blk, head, out, keys);
+    GIR_LAUNCH(g, "k_single_edit");
+    return GIR_OK;
+}
 
 int store_free(gir_dev* g, DevCSR& c) {
     dev_free(g, c.beg);

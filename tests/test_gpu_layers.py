@@ -397,3 +397,49 @@ def test_ingest_and_sync_match_reference(pkg, orc, s16):
     _oracle_match(pkg, orc, d, g.V, cb, ca, "after apply_batch on pending batches")
     ref.close()
     d.close()
+
+
+def test_single_edge_in_place_edits_keep_the_store_exact(pkg, orc):
+    """One-op batches edit the forward, backward and symmetric rows in place (one CTA) while a row
+    has room, and fall back to the batch merge when it has none: 14 inserts into one row (its
+    slack runs out), deletions, re-inserts, no-ops and invalid ops, on a graph with stored weights.
+    After every op the three CSRs equal the oracle's; at the end SSSP over the stored weights
+    (new edges take the hash weight, the default weight rule) equals the oracle's Dijkstra."""
+    g = pkg.graphs.rmat(10, seed=77)
+    V = g.V
+    fb, fa = orc.normalize(V, g.fw_beg, g.fw_adj)
+    w = {}
+    rows = np.repeat(np.arange(V), np.diff(g.fw_beg))
+    for r, x, wt in zip(rows, g.fw_adj, g.w):
+        w[(int(r), int(x))] = int(wt)
+    d = pkg.DeviceGraph.from_graph(g)
+    d.build(pkg.native.LAYER_ALL)
+    deg = np.diff(fb)
+    small = int(np.nonzero(deg == 4)[0][0])  # capacity 8: room for 4 inserts, then the fallback
+    rng = np.random.default_rng(3)
+    ops = [(small, int(x), 1) for x in rng.choice(V, 14, replace=False) if x != small]
+    ops += [(int(rows[j]), int(g.fw_adj[j]), 0) for j in rng.choice(len(g.fw_adj), 10, replace=False)]
+    ops += [ops[0], (ops[1][0], ops[1][1], 0), (ops[1][0], ops[1][1], 1), (5, 5, 1), (-1, 3, 1), (3, V, 0)]
+    for i, (u, v, ins) in enumerate(ops):
+        d.apply_batch(np.array([u], np.int32), np.array([v], np.int32), np.array([ins], np.uint8))
+        fb, fa, _, _ = orc.apply_batch(V, fb, fa, [u], [v], [ins])
+        if 0 <= u < V and 0 <= v < V and u != v:
+            if ins:
+                w.setdefault((u, v), orc.edge_weight(u, v))
+            else:
+                w.pop((u, v), None)
+        cb, ca = d.csr(0)
+        np.testing.assert_array_equal(cb, fb, err_msg=f"op {i}: fw offsets")
+        np.testing.assert_array_equal(ca, fa, err_msg=f"op {i}: fw")
+        bb, ba = orc.transpose(V, fb, fa)
+        np.testing.assert_array_equal(d.csr(1)[1], ba, err_msg=f"op {i}: bw")
+        sb, sa = orc.sym(V, fb, fa, bb, ba)
+        np.testing.assert_array_equal(d.csr(2)[1], sa, err_msg=f"op {i}: sym")
+    _oracle_match(pkg, orc, d, V, fb, fa, "after the single ops")
+    rows = np.repeat(np.arange(V), np.diff(fb))
+    wf = np.array([w[(int(r), int(x))] for r, x in zip(rows, fa)], np.uint32)
+    src = pkg.graphs.sources(V, 5, 9)
+    ds = d.sssp(src, delta=16, weights=pkg.native.WEIGHT_STORED)
+    for i, s in enumerate(src):
+        np.testing.assert_array_equal(ds[i], orc.sssp(V, fb, fa, [s], w=wf), err_msg=f"stored-weight SSSP from {s}")
+    d.close()

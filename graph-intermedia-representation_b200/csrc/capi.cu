@@ -1161,7 +1161,12 @@ int gir_dev_set_schedule(gir_dev_t* g, int mode) {
 int gir_dev_set_param(gir_dev_t* g, int which, double value) {
     if (!g) return GIR_ERR_INVALID;
     if (which < 0 || which >= GIR_PARAM_COUNT) return fail(g, GIR_ERR_INVALID, "unknown parameter");
-    if (!(value > 0) && which != GIR_PARAM_PROFILE) return fail(g, GIR_ERR_INVALID, "parameters are positive");
+    if (which == GIR_PARAM_PIVOT) {
+        if (value != -1.0 && !(value == 0.0 || value == 1.0 || value == 2.0 || value == 3.0))
+            return fail(g, GIR_ERR_INVALID, "pivot rule: -1 (the schedule decides) or 0..3");
+    } else if (!(value > 0) && which != GIR_PARAM_PROFILE) {
+        return fail(g, GIR_ERR_INVALID, "parameters are positive");
+    }
     if (which == GIR_PARAM_BLOCK && ((int)value % 32 != 0 || value > 1024)) return fail(g, GIR_ERR_INVALID, "block: multiple of 32, <= 1024");
     g->params[which] = value;
     if (which == GIR_PARAM_SMALL_DEG || which == GIR_PARAM_LARGE_DEG) g->bins_valid = false;

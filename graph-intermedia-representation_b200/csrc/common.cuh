@@ -170,7 +170,7 @@ struct gir_dev {
 
     // Schedule
     int schedule = GIR_SCHEDULE_FIXED;
-    double params[GIR_PARAM_COUNT] = {15.0, 18.0, 16.0, 256.0, 32.0, 4096.0, 4.0, 0.0};
+    double params[GIR_PARAM_COUNT] = {15.0, 18.0, 16.0, 256.0, 32.0, 4096.0, 4.0, 0.0, -1.0};
     cudaEvent_t pev0 = nullptr, pev1 = nullptr;  // main-kernel timing (GIR_PARAM_PROFILE)
     gir::DevBuf sched_w;              // MLP parameters (fp32)
     gir::DevBuf sched_io;             // one decision's features and logits
@@ -327,6 +327,10 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
 
 // ---- schedule network (sched.cu) ----
 int sched_choose_delta(gir_dev* g, const float* features, uint64_t* delta);
+// The SCC build's forward-backward pivot rule (0..3, see GIR_PARAM_PIVOT) from the network, with
+// the fixed rule 0 when its margin is small; features from sched_scc_features.
+int sched_choose_pivot(gir_dev* g, const float* features, int* rule);
+void sched_scc_features(const gir_dev* g, double active, double active_edges, double max_score, float* out);
 // Enqueues the device decision of the next BFS level's direction: reads the frontier's pairs and
 // out-edges at cnt[i_pairs] / cnt[i_medges], writes the direction (0 top-down, 1 bottom-up) to
 // cnt[i_dir] and the GIR_SCHED_IN features (floats) from cnt[i_feat] on.

@@ -32,7 +32,7 @@ constexpr int kWarps = kBlock / 32;
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-enum { C_Q = 0, C_ACT = 1, C_ROOTS = 2, C_PIV = 3, C_N = 8 };
+enum { C_Q = 0, C_ACT = 1, C_ROOTS = 2, C_PIV = 3, C_ACT_E = 4, C_N = 8 };
 
 // Active in/out degree counts (self-loops excluded) and the first trim frontier.
 __global__ void k_trim_init(int64_t V, CSRView fw, CSRView bw, int32_t* label, int32_t* indeg, int32_t* outdeg,
@@ -117,15 +117,20 @@ __global__ void k_trim2_apply(int64_t V, const int32_t* partner, int32_t* label,
     if (lane_id() == 0 && c) atomicAdd(n_pairs, c);
 }
 
-// Pivot: the unassigned vertex with the largest out x in degree (ties: larger id).
-__global__ void k_pivot(int64_t V, const int32_t* label, const int32_t* indeg, const int32_t* outdeg,
+// Pivot: the unassigned vertex with the largest score (ties: larger id). Rules: 0 out x in
+// degree (iSpan's pivot_selection_from_fq, gir_constructor/includes/scc_cpu/scc_common.h:98-146,
+// the fixed schedule), 1 out + in, 2 in-degree. Also counts the unassigned vertices (C_ACT) and
+// their edges (C_ROOTS + 1: out-degrees summed), the schedule's features.
+__global__ void k_pivot(int64_t V, const int32_t* label, const int32_t* indeg, const int32_t* outdeg, int rule,
                         unsigned long long* cnt) {
     unsigned long long best = 0;
-    unsigned long long act = 0;
+    unsigned long long act = 0, act_e = 0;
     GRID_STRIDE(v, V) {
         if (label[v] != -1) continue;
         ++act;
-        const unsigned long long s = (unsigned long long)(uint32_t)outdeg[v] * (unsigned long long)(uint32_t)indeg[v];
+        act_e += (uint32_t)outdeg[v];
+        const unsigned long long o = (uint32_t)outdeg[v], i = (uint32_t)indeg[v];
+        const unsigned long long s = rule == 1 ? o + i : (rule == 2 ? i : o * i);
         const unsigned long long k = ((s < (1ull << 31) ? s : (1ull << 31)) << 32) | (unsigned long long)v;
         if (k + 1 > best) best = k + 1;
     }
@@ -133,10 +138,12 @@ __global__ void k_pivot(int64_t V, const int32_t* label, const int32_t* indeg, c
         const unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
         best = t > best ? t : best;
         act += __shfl_xor_sync(0xffffffffu, act, o);
+        act_e += __shfl_xor_sync(0xffffffffu, act_e, o);
     }
     if (lane_id() == 0) {
         if (best) atomicMax(&cnt[C_PIV], best);
         if (act) atomicAdd(&cnt[C_ACT], act);
+        if (act_e) atomicAdd(&cnt[C_ACT_E], act_e);
     }
 }
 
@@ -397,11 +404,34 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
     // 2. forward-backward from the max-degree pivot
     GIR_CUDA(g, cudaMemsetAsync(mark, 0, sizeof(int32_t) * V, g->stream));
     GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
-    k_pivot<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, indeg, outdeg, cnt);
+    k_pivot<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, indeg, outdeg, 0, cnt);
     GIR_LAUNCH(g, "k_pivot");
     GIR_CUDA(g, cudaMemcpyAsync(lp.hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-    if (lp.hc[C_PIV] != 0) {
+    // The pivot rule: forced by GIR_PARAM_PIVOT, else the fixed max out x in degree or the
+    // schedule network (rule 3: no forward-backward pass, colour propagation does everything).
+    // Any rule gives the same SCCs; only the time differs.
+    int rule = (int)g->params[GIR_PARAM_PIVOT];
+    {
+        float feat[GIR_SCHED_IN];
+        sched_scc_features(g, (double)lp.hc[C_ACT], (double)lp.hc[C_ACT_E],
+                           lp.hc[C_PIV] ? (double)((lp.hc[C_PIV] - 1) >> 32) : 0.0, feat);
+        if (rule < 0) {
+            rule = 0;
+            if (g->schedule == GIR_SCHEDULE_LEARNED && g->sched_loaded) GIR_TRY(sched_choose_pivot(g, feat, &rule));
+        }
+        g->trace_x.clear();
+        g->trace_y.clear();
+        sched_trace(g, feat, 8 + rule);
+    }
+    if (rule == 1 || rule == 2) {
+        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
+        k_pivot<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, label, indeg, outdeg, rule, cnt);
+        GIR_LAUNCH(g, "k_pivot");
+        GIR_CUDA(g, cudaMemcpyAsync(lp.hc, cnt, sizeof(unsigned long long) * C_N, cudaMemcpyDeviceToHost, g->stream));
+        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+    }
+    if (rule != 3 && lp.hc[C_PIV] != 0) {
         const int32_t pivot = (int32_t)((lp.hc[C_PIV] - 1) & 0xffffffffULL);
         const int32_t epoch = 1;
         // forward reach (marks), seeded with the pivot

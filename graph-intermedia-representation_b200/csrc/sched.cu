@@ -3,8 +3,11 @@
 //
 // It only picks schedule choices, never results: logits 0..1 choose the BFS direction of the
 // next level (top-down / bottom-up), logits 2..7 the Delta-stepping bucket width (one of
-// kDeltaChoices). The fixed heuristics of the reference (alpha = 15, beta = 18,
-// gir_query.cpp:161-168; Delta = 16, gir.h:215) are the fallback when no network is loaded.
+// kDeltaChoices), logits 8..11 the forward-backward pivot rule of the SCC build (max out x in
+// degree, max out + in, max in-degree, or no forward-backward pass). The fixed heuristics (alpha =
+// 15, beta = 18, gir_query.cpp:161-168; Delta = 16, gir.h:215; the max out x in pivot of iSpan,
+// gir_constructor/includes/scc_cpu/scc_common.h:98-146) are the fallback when no network is
+// loaded, and for the direction and the pivot also when the network's margin is small.
 //
 // Feature vectors (built by the callers in bfs.cu / sssp.cu, all scaled to O(1)):
 //   BFS level:  [log2(nf / V) / 8, log2(mf / mu) / 8, log2(mu / E) / 8, log2(mf / E) / 8,
@@ -15,6 +18,8 @@
 //               better pair of thresholds, a simple function of the inputs.
 //   SSSP query: [log2(E / V + 1) / 8, log2(mean weight + 1) / 16, log2(max weight + 1) / 16,
 //                log2(V) / 32, lanes / 64, 0, 0, 1]
+//   SCC pivot:  [log2(E / V + 1) / 8, log2(active / V) / 8, log2(active edges / active + 1) / 8,
+//                log2(V) / 32, log2(max out x in + 1) / 64, 0, 0, 0.5], after trimming
 // A direction is taken from the network only when its two logits differ by at least
 // kDirMargin; otherwise the fixed switch decides.
 // Parameter layout: W1[HID][IN], b1[HID], W2[OUT][HID], b2[OUT].
@@ -216,6 +221,27 @@ void sched_trace(gir_dev* g, const float* x, int32_t y) {
     if (g->trace_y.size() >= (1u << 20)) return;  // bounded
     g->trace_x.insert(g->trace_x.end(), x, x + IN);
     g->trace_y.push_back(y);
+}
+
+void sched_scc_features(const gir_dev* g, double active, double active_edges, double max_score, float* out) {
+    const double V = (double)(g->V > 0 ? g->V : 1), E = (double)g->fw.E + 1.0;
+    const double tiny = 1.0 / 4294967296.0;
+    out[0] = (float)(std::log2(E / V + 1.0) / 8.0);
+    out[1] = (float)(std::log2(active / V + tiny) / 8.0);
+    out[2] = (float)(std::log2(active_edges / (active + 1.0) + 1.0) / 8.0);
+    out[3] = (float)(std::log2(V) / 32.0);
+    out[4] = (float)(std::log2(max_score + 1.0) / 64.0);
+    out[5] = 0.f;
+    out[6] = 0.f;
+    out[7] = 0.5f;  // task: SCC pivot rule
+}
+
+int sched_choose_pivot(gir_dev* g, const float* features, int* rule) {
+    int c = 8;
+    float margin = 0.f;
+    GIR_TRY(decide(g, features, 8, 12, &c, &margin));
+    *rule = margin >= kPivotMargin ? c - 8 : 0;
+    return GIR_OK;
 }
 
 int sched_choose_delta(gir_dev* g, const float* features, uint64_t* delta) {

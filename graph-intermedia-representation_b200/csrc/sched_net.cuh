@@ -13,6 +13,9 @@ constexpr int NP = HID * IN + HID + OUT * HID + OUT;
 // A BFS direction is taken from the network only when its two logits differ by at least this;
 // otherwise the fixed switch decides.
 constexpr float kDirMargin = 8.0f;
+// The pivot rule is taken from the network only when its best logit leads the runner-up by at
+// least this; otherwise the fixed rule (max out x in degree) is used.
+constexpr float kPivotMargin = 1.0f;
 
 struct Layout {
     const float *W1, *b1, *W2, *b2;

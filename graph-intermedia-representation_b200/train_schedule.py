@@ -7,9 +7,12 @@ high-diameter lattices), the method sweeps its own choices and keeps the fastest
         and lane count; the sample is the group's feature row (sssp features) with the class of
         the fastest Delta;
   BFS   the direction-switch thresholds (alpha, beta) over a grid; the samples are the
-        per-level feature rows of the fastest setting's run with the direction it took.
+        per-level feature rows of the fastest setting's run with the direction it took;
+  SCC   the forward-backward pivot rule (max out x in degree, max out + in, max in-degree, no
+        forward-backward pass), per graph; the sample is the build's feature row with the class
+        of the fastest rule.
 
-The network (8 features -> 32 tanh -> 8 logits) is then trained on the GPU by this library's
+The network (8 features -> 32 tanh -> 12 logits) is then trained on the GPU by this library's
 own forward/backward/SGD kernels (gir_dev_sched_train), and its weights are written to
 schedule_weights.npy beside this file, where DeviceGraph.use_learned_schedule() loads them.
 Results never depend on the schedule: every choice gives bit-identical levels and distances.
@@ -92,6 +95,22 @@ def main():
                 ys.append(2 + best)
             print(json.dumps(log[-1]), flush=True)
         if wk == "hash" or g.name.startswith("lattice"):
+            # SCC build: the four pivot rules (same SCCs; only the time differs)
+            times, feat = [], None
+            for rule in range(4):
+                d.set_param(native.PARAM_PIVOT, rule)
+                d.build(native.LAYER_SCC)
+                times.append(timed(lambda: d.build(native.LAYER_SCC)))
+                if feat is None:
+                    feat = d.sched_trace()[0][0]
+            d.set_param(native.PARAM_PIVOT, -1)
+            best = int(np.argmin(times))
+            log.append({"graph": g.name, "scc_ms_by_pivot_rule": [round(1e3 * t, 2) for t in times], "best_rule": best})
+            rng = np.random.default_rng(100 + len(log))
+            for _ in range(40):
+                xs.append(feat * (1 + 0.01 * rng.standard_normal(feat.shape)).astype(np.float32))
+                ys.append(8 + best)
+            print(json.dumps(log[-1]), flush=True)
             for lanes in (1, 8, 64):
                 src = torch.from_numpy(pkg.graphs.sources_with_edges(g, lanes, 9 + lanes)).to("cuda:0")
                 out = torch.empty((lanes, g.V), dtype=torch.int32, device="cuda:0")
@@ -123,7 +142,8 @@ def main():
     loss0 = d.sched_grad(x, y)[1]
     loss = d.sched_train(x, y, steps=args.steps, lr=args.lr)
     logits = d.sched_forward(x)
-    pred = np.where(y < 2, np.argmax(logits[:, :2], 1), 2 + np.argmax(logits[:, 2:], 1))
+    pred = np.where(y < 2, np.argmax(logits[:, :2], 1),
+                    np.where(y < 8, 2 + np.argmax(logits[:, 2:8], 1), 8 + np.argmax(logits[:, 8:], 1)))
     acc = float((pred == y).mean())
     w = d.sched_get_weights()
     d.close()

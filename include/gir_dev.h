@@ -242,7 +242,11 @@ enum {
     GIR_PARAM_CTAS_PER_SM = 6,  /* grid size = SMs x this */
     GIR_PARAM_PROFILE = 7,      /* 1: time every launch of the main traversal kernel with CUDA events
                                    (gir_dev_query_stats main_ms / main_launches); 0: off */
-    GIR_PARAM_COUNT = 8
+    GIR_PARAM_PIVOT = 8,        /* forward-backward pivot rule of the SCC build: -1 the schedule decides
+                                   (fixed: max out x in degree; learned: the network), or forced: 0 max
+                                   out x in, 1 max out + in, 2 max in-degree, 3 no forward-backward pass
+                                   (colour propagation only) */
+    GIR_PARAM_COUNT = 9
 };
 int gir_dev_set_param(gir_dev_t* g, int which, double value);
 int gir_dev_get_param(gir_dev_t* g, int which, double* value);
@@ -295,7 +299,7 @@ int gir_dev_bfs_noalloc(const int64_t* beg, const int32_t* adj, int64_t n_adj, i
 
 /* Schedule network: a 2-layer MLP (GIR_SCHED_IN features -> GIR_SCHED_HID tanh -> GIR_SCHED_OUT
  * logits), fp32, trained and evaluated by this library's own CUDA kernels. */
-enum { GIR_SCHED_IN = 8, GIR_SCHED_HID = 32, GIR_SCHED_OUT = 8 };
+enum { GIR_SCHED_IN = 8, GIR_SCHED_HID = 32, GIR_SCHED_OUT = 12 };
 int gir_dev_sched_set_weights(gir_dev_t* g, const float* params, int64_t n_params);
 int gir_dev_sched_get_weights(gir_dev_t* g, float* params, int64_t n_params);
 int64_t gir_dev_sched_param_count(void);

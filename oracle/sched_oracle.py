@@ -1,13 +1,13 @@
 """CPU restatement of the schedule network -- TEST INFRASTRUCTURE ONLY.
 
 The network of graph-intermedia-representation_b200/csrc/sched.cu in float64 numpy: 8 features
--> 32 tanh units -> 8 logits, parameters laid out W1[32][8], b1[32], W2[8][32], b2[8]; loss =
+-> 32 tanh units -> 12 logits, parameters laid out W1[32][8], b1[32], W2[12][32], b2[12]; loss =
 mean softmax cross-entropy. The GPU tests check the device forward pass and gradient against it.
 (The schedule network has no counterpart in the reference, which uses fixed thresholds.)
 """
 import numpy as np
 
-IN, HID, OUT = 8, 32, 8
+IN, HID, OUT = 8, 32, 12
 NP = HID * IN + HID + OUT * HID + OUT
 
 

@@ -59,9 +59,10 @@ def parse():
                    help="instead of the bench: the 41.6M-vertex / 1.47B-edge R-MAT (seed 5, weights U[1,1023]), "
                         "WCC + SCC build, then ROUNDS x (1M-edge batch 60/40 + 32 BFS + 32 SSSP), checked by "
                         "the size-independent certificates; one JSON line")
-    p.add_argument("--only", choices=["bfs", "sssp", "build"], default=None,
-                   help="profiling runs: one call of one query kind (or the three layer builds and one "
-                        "10K update batch), no timing and no JSON line")
+    p.add_argument("--only", choices=["bfs", "sssp", "build", "reach", "bc", "incr", "single"], default=None,
+                   help="profiling runs: one call of one query kind (or the three layer builds and one 10K "
+                        "update batch; 64K reachability pairs; betweenness over 64 sources; a 10K-op batch "
+                        "and the incremental BFS / SSSP updates after it; 20 single-edge updates), no timing")
     return p.parse_args()
 
 
@@ -88,6 +89,39 @@ def run_only(args):
         d.apply_batch(u, v, ins)
         torch.cuda.synchronize()
         print(json.dumps({"only": "build", "workload": args.workload, **d.counts()}))
+        d.close()
+        return
+    if args.only in ("reach", "bc", "incr", "single"):
+        import numpy as np
+        d.build(pkg.native.LAYER_ALL)
+        if args.only == "reach":
+            rng = np.random.default_rng(77)
+            n = 1 << 16
+            ru = torch.from_numpy(rng.integers(0, g.V, n).astype(np.int32)).to("cuda:0")
+            rv = torch.from_numpy(rng.integers(0, g.V, n).astype(np.int32)).to("cuda:0")
+            d.reachable(ru, rv, out=torch.empty(n, dtype=torch.uint8, device="cuda:0"))
+        elif args.only == "bc":
+            d.bc(src, out=torch.empty(g.V, dtype=torch.float64, device="cuda:0"))
+        elif args.only == "incr":
+            s0 = int(src[0].item())
+            d.inc_track(s0, False)
+            d.inc_track(s0, True)
+            u, v, ins = pkg.graphs.updates(g, 5000, 5000, 6)
+            d.apply_batch(u, v, ins)
+            d.inc_update(False)
+            d.inc_update(True)
+        else:
+            rng = np.random.default_rng(5)
+            cb, ca = d.csr(0)
+            for i in range(20):
+                a = int(rng.integers(g.V))
+                while cb[a + 1] == cb[a]:
+                    a = int(rng.integers(g.V))
+                b = int(ca[cb[a] + rng.integers(cb[a + 1] - cb[a])]) if i % 2 == 0 else int(rng.integers(g.V))
+                if a != b:
+                    d.apply_batch(np.array([a], np.int32), np.array([b], np.int32), np.array([i % 2], np.uint8))
+        torch.cuda.synchronize()
+        print(json.dumps({"only": args.only, "workload": args.workload, **d.counts()}))
         d.close()
         return
     if args.only == "bfs":

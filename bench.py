@@ -316,6 +316,31 @@ def reference_instance(pkg, d):
                  "input": f"int32 four-array CSR of the current graph (V={d.V}, E={len(ca)}), host memory"}
 
 
+def stream_protocol_section(pkg, with_reference, scale=18, batch=10000, batches=10):
+    """The reference's streaming protocol (experiments/baselines/gir/gir_stream.cpp): one exported
+    protocol (R-MAT scale `scale`, half its edges loaded, insert / delete / mixed streams), run by
+    this package's gir_stream on the GPU and by the reference's own driver on the host cores, in
+    the applyBatch, lazy (ingestBatch + sync) and incremental modes. Rows: mutation MEPS per
+    stream, BFS and SSSP end-to-end ms per batch, the lazy mode's sync ms, incremental mismatches."""
+    import tempfile
+    st = importlib.import_module("graph-intermedia-representation_b200.stream")
+    ref_driver = os.path.join(ROOT, "oracle", "_ref", "gir_stream_ref")
+    g = pkg.graphs.rmat(scale, seed=8, permute=True, weights=None)
+    keep = ("mutation_MEPS", "endtoend_ms", "sync_", "inc_mismatch")
+    out = {"graph": f"R-MAT scale {scale}, V={g.V}", "batch": batch, "batches": batches}
+    with tempfile.TemporaryDirectory() as d:
+        out["protocol"] = st.export_protocol(g, d, ops_per_stream=batch * batches)
+        out["protocol"].pop("sources", None)
+        systems = [("device", st.DRIVER)] + ([("reference", ref_driver)] if with_reference and os.path.exists(ref_driver) else [])
+        for name, binary in systems:
+            res = {}
+            for mode in ("", "lazy", "inc"):
+                rows = st.run_driver(binary, d, f"rmat_s{scale}", os.path.join(d, f"{name}.csv"), batch, batches, mode)
+                res[mode or "fmu"] = {r["metric"]: round(r["value"], 4) for r in rows if any(k in r["metric"] for k in keep)}
+            out[name] = res
+    return out
+
+
 def cpu_model():
     """The host CPU's model name and logical core count."""
     try:
@@ -819,6 +844,10 @@ def run_ours(args):
                               "true_fraction": float(rout.float().mean().item())}
         if rep is not None:
             extra["replicas_agree_checksum"] = rep.check_agree()
+
+    # the reference's streaming protocol, both drivers on the same protocol files
+    if not args.no_updates and rank == 0:
+        extra["stream_protocol"] = stream_protocol_section(pkg, with_reference=world == 1 and not args.no_cpu)
 
     # batched source sets interleaved with uneven update batches (on the updated graph)
     if not args.no_batched and not args.no_updates:

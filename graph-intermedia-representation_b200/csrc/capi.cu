@@ -1164,6 +1164,11 @@ int gir_dev_set_param(gir_dev_t* g, int which, double value) {
     if (which == GIR_PARAM_PIVOT) {
         if (value != -1.0 && !(value == 0.0 || value == 1.0 || value == 2.0 || value == 3.0))
             return fail(g, GIR_ERR_INVALID, "pivot rule: -1 (the schedule decides) or 0..3");
+    } else if (which == GIR_PARAM_LANE_BITS) {
+        if (!(value == 0.0 || value == 16.0 || value == 32.0 || value == 64.0))
+            return fail(g, GIR_ERR_INVALID, "lane bits: 0 (the library decides), 16, 32 or 64");
+    } else if (which == GIR_PARAM_LANE_ORDER) {
+        if (!(value == 0.0 || value == 1.0)) return fail(g, GIR_ERR_INVALID, "lane order: 0 or 1");
     } else if (!(value > 0) && which != GIR_PARAM_PROFILE) {
         return fail(g, GIR_ERR_INVALID, "parameters are positive");
     }

@@ -170,7 +170,7 @@ struct gir_dev {
 
     // Schedule
     int schedule = GIR_SCHEDULE_FIXED;
-    double params[GIR_PARAM_COUNT] = {15.0, 18.0, 16.0, 256.0, 32.0, 4096.0, 4.0, 0.0, -1.0};
+    double params[GIR_PARAM_COUNT] = {15.0, 18.0, 16.0, 256.0, 32.0, 4096.0, 4.0, 0.0, -1.0, 0.0, 1.0};
     cudaEvent_t pev0 = nullptr, pev1 = nullptr;  // main-kernel timing (GIR_PARAM_PROFILE)
     gir::DevBuf sched_w;              // MLP parameters (fp32)
     gir::DevBuf sched_io;             // one decision's features and logits

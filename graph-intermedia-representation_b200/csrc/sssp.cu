@@ -839,7 +839,7 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
     // the placement of the queries changes, never their results.
     std::vector<int64_t> order((size_t)n_sets);
     for (int64_t i = 0; i < n_sets; ++i) order[i] = i;
-    if (n_sets > 1) {
+    if (n_sets > 1 && g->params[GIR_PARAM_LANE_ORDER] != 0.0) {
         GIR_TRY(hub_order(g, hash));
         int64_t* sb = nullptr;
         GIR_TRY(ensure_n(g, g->sssp_sets, 2 * n_sets + 1, &sb));
@@ -857,13 +857,16 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
     GIR_TRY(sssp_work(g, wk, ws.E));
     int64_t* lanes = nullptr;  // lane ranges (2 per lane), then output rows (1 per lane)
     GIR_TRY(ensure_n(g, g->sssp_lanes, 3 * 64, &lanes));
-    // Lane distance width: 32 bits when every finite distance fits ((V - 1) x max weight), else
-    // 64; 16 bits first when the distances to the hub suggest short paths and no 16-bit run of
-    // this handle has overflowed (an overflow reruns the group with the wider type, so the width
-    // never changes a result).
+    // Lane distance width (GIR_PARAM_LANE_BITS): by default 32 bits when every finite distance
+    // fits ((V - 1) x max weight), else 64. 16 bits are taken only when asked for, and only while
+    // no 16-bit run of this handle has overflowed (an overflow reruns the group wider, so the
+    // width never changes a result): their minimum is a compare-and-swap on the 32-bit word the
+    // lane shares with its neighbour, and neighbouring lanes active together make those swaps
+    // retry (measured slower than 32-bit atomicMin on the LJ-shape graph).
     const double wmax = g->wstat[mi][1] > 0 ? g->wstat[mi][1] : 4294967295.0;
-    const bool fits32 = (double)V * wmax < 4294967295.0;
-    const bool try16 = g->hub_valid[mi] && !g->narrow16_failed[mi] && g->hub_max[mi] * 4 < 0xffffull;
+    const int bits = (int)g->params[GIR_PARAM_LANE_BITS];
+    const bool fits32 = bits != 64 && (double)V * wmax < 4294967295.0;
+    const bool try16 = bits == 16 && !g->narrow16_failed[mi];
     GIR_CUDA(g, cudaEventRecord(g->ev0, g->stream));
     GIR_CUDA(g, cudaMemsetAsync(wk.cnt, 0, sizeof(unsigned long long) * S_N, g->stream));
     std::vector<int64_t> lh(3 * 64);

@@ -22,7 +22,7 @@ LABEL_WCC, LABEL_SCC, LABEL_BLOCK, LABEL_BCNT, LABEL_SCC_RANK = 0, 1, 2, 3, 4
 WEIGHT_HASH, WEIGHT_STORED = 0, 1
 SCHEDULE_FIXED, SCHEDULE_LEARNED = 0, 1
 (PARAM_ALPHA, PARAM_BETA, PARAM_DELTA, PARAM_BLOCK, PARAM_SMALL_DEG, PARAM_LARGE_DEG, PARAM_CTAS_PER_SM,
- PARAM_PROFILE, PARAM_PIVOT) = range(9)
+ PARAM_PROFILE, PARAM_PIVOT, PARAM_LANE_BITS, PARAM_LANE_ORDER) = range(11)
 SCHED_IN, SCHED_HID, SCHED_OUT = 8, 32, 12
 
 # Every symbol include/gir_dev.h declares (checked by the CPU test suite).

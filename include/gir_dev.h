@@ -246,7 +246,12 @@ enum {
                                    (fixed: max out x in degree; learned: the network), or forced: 0 max
                                    out x in, 1 max out + in, 2 max in-degree, 3 no forward-backward pass
                                    (colour propagation only) */
-    GIR_PARAM_COUNT = 9
+    GIR_PARAM_LANE_BITS = 9,    /* SSSP lane distances: 0 the library decides (32 bits when every finite
+                                   distance fits, else 64), or 16 / 32 / 64; 16 bits run optimistically
+                                   and a group that meets a longer distance is rerun wider */
+    GIR_PARAM_LANE_ORDER = 10,  /* SSSP lanes: 1 ordered by the sources' distance to the largest-in-degree
+                                   vertex (lanes active in the same buckets share sectors), 0 query order */
+    GIR_PARAM_COUNT = 11
 };
 int gir_dev_set_param(gir_dev_t* g, int which, double value);
 int gir_dev_get_param(gir_dev_t* g, int which, double* value);

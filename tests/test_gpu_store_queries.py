@@ -294,10 +294,16 @@ def test_sssp_lane_order_and_groups_map_back_to_query_rows(pkg, orc, s16):
     src = pkg.graphs.sources(g.V, 70, 9)
     src[5] = src[40]
     src[66] = g.V + 3
-    for weights, w in ((pkg.native.WEIGHT_HASH, None), (pkg.native.WEIGHT_STORED, g.w)):
-        ds = d.sssp(src, delta=16, weights=weights)
-        for i, s in enumerate(src):
-            np.testing.assert_array_equal(ds[i], orc.sssp(g.V, fb, fa, [s], w=w), err_msg=f"query {i}, source {s}")
+    exp = {0: [orc.sssp(g.V, fb, fa, [s]) for s in src], 1: [orc.sssp(g.V, fb, fa, [s], w=g.w) for s in src]}
+    for bits in (0, 16, 32, 64):
+        for order in (1, 0):
+            d.set_param(pkg.native.PARAM_LANE_BITS, bits)
+            d.set_param(pkg.native.PARAM_LANE_ORDER, order)
+            for weights in (pkg.native.WEIGHT_HASH, pkg.native.WEIGHT_STORED):
+                ds = d.sssp(src, delta=16, weights=weights)
+                for i, s in enumerate(src):
+                    np.testing.assert_array_equal(ds[i], exp[weights][i],
+                                                  err_msg=f"query {i}, source {s}, {bits} bits, order {order}")
     d.close()
 
 
@@ -315,6 +321,7 @@ def test_sssp_16bit_lane_overflow_reruns_wider(pkg, orc):
     g = pkg.graphs.from_edges(V, np.array(es), np.array(ed), np.array(ew, np.uint32))
     fb, fa = orc.normalize(g.V, g.fw_beg, g.fw_adj)
     d = pkg.DeviceGraph.from_graph(g)
+    d.set_param(pkg.native.PARAM_LANE_BITS, 16)
     src = np.array([1, 100, 5, 0, 150], np.int32)
     for _ in range(2):  # the second call starts from the handle's remembered overflow
         ds = d.sssp(src, delta=16, weights=pkg.native.WEIGHT_STORED)

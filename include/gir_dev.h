@@ -179,7 +179,8 @@ int gir_dev_batch_plan(gir_dev_t* g, int32_t* plan3);
  * GIR_PARAM_CTAS_PER_SM in {2, 4, 8}, GIR_PARAM_SMALL_DEG in {8, 32, 128} and GIR_PARAM_LARGE_DEG
  * in {1024, 4096, 32768}, best of `reps` calls each, and keeps the fastest setting on the handle
  * (read it back with gir_dev_get_param). The parameters shape launches only, so results never
- * change. *best_ms (may be NULL) = the winner's device time per call. */
+ * change. *best_ms (may be NULL) = the winner's device time per call. Queues need no tuning: each
+ * is sized for its exact bound (V entries, or the SSSP items' bound), allocated once per handle. */
 int gir_dev_autotune(gir_dev_t* g, const int32_t* srcs, int64_t n_src, int reps, double* best_ms);
 
 /* GIR::reachable (gir_query.cpp:789-825) for a batch: out[i] = 1 iff v[i] is reachable from u[i]
@@ -236,7 +237,8 @@ enum {
     GIR_PARAM_ALPHA = 0,        /* top-down -> bottom-up when frontier edges * alpha > unexplored */
     GIR_PARAM_BETA = 1,         /* bottom-up -> top-down when frontier * beta < vertices */
     GIR_PARAM_DELTA = 2,        /* default Delta of the fixed schedule */
-    GIR_PARAM_BLOCK = 3,        /* accepted and stored; the kernels use fixed 256-thread CTAs */
+    GIR_PARAM_BLOCK = 3,        /* reserved, no effect: every kernel's CTA size is fixed by its shared-memory
+                                   layout (the launch shape the autotuner varies is CTAs per SM) */
     GIR_PARAM_SMALL_DEG = 4,    /* degree bin: thread per vertex below this in-degree */
     GIR_PARAM_LARGE_DEG = 5,    /* degree bin: CTA per vertex from this in-degree on */
     GIR_PARAM_CTAS_PER_SM = 6,  /* grid size = SMs x this */

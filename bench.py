@@ -341,6 +341,31 @@ def stream_protocol_section(pkg, with_reference, scale=18, batch=10000, batches=
     return out
 
 
+def two_level_section(pkg, d, ref, native, n_src=4):
+    """The reference's two-level queries (GIR::bfsTwoLevel / ssspTwoLevel, gir_query.cpp:604-722: a
+    wavefront over the condensation DAG with block tasks in the source SCC) beside its flat bfs /
+    sssp and the device's flat single-source query, from the same sources on the same graph
+    (host wall clock per source; delta 16, hash weights); every result must agree."""
+    import numpy as np
+    fb, fa = d.csr(0)
+    src = pkg.graphs.sources_with_edges(pkg.graphs.Graph(d.V, fb.astype(np.int32), fa, None, None), n_src, 23)
+    t = {"ref_bfs": 0.0, "ref_bfs_two_level": 0.0, "ref_sssp": 0.0, "ref_sssp_two_level": 0.0,
+         "device_bfs": 0.0, "device_sssp": 0.0}
+    same = True
+    d.bfs(src[:1])
+    d.sssp(src[:1], delta=DELTA)
+    for s in src.tolist():
+        t0 = time.perf_counter(); a = ref.bfs(s); t1 = time.perf_counter(); b = ref.bfs_two_level(s)
+        t2 = time.perf_counter(); c = ref.sssp(s, DELTA); t3 = time.perf_counter(); e = ref.sssp_two_level(s, DELTA)
+        t4 = time.perf_counter(); x = d.bfs([s])[0]; t5 = time.perf_counter(); y = d.sssp([s], delta=DELTA)[0]
+        t6 = time.perf_counter()
+        for k, dt in zip(t, (t1 - t0, t2 - t1, t3 - t2, t4 - t3, t5 - t4, t6 - t5)):
+            t[k] += dt * 1e3 / len(src)
+        same &= bool(np.array_equal(a, b) and np.array_equal(a, x) and np.array_equal(c, e) and np.array_equal(c, y))
+    return {"ms_per_source": {k: round(v, 3) for k, v in t.items()}, "identical": same, "sources": len(src),
+            "note": "host wall clock per single-source call; device calls include the copy of the V-entry result row"}
+
+
 def cpu_model():
     """The host CPU's model name and logical core count."""
     try:
@@ -819,6 +844,7 @@ def run_ours(args):
                 "cpu": cpu_model(), "note": "GIR::applyBatch of the reference compiled from its sources, the same "
                                             "batches on the same graph, host wall clock"}
             extra["full_size_parity"] = parity_vs_reference(pkg, d, ref, native)
+            extra["two_level"] = two_level_section(pkg, d, ref, native)
         # reachability (GIR::reachable) for 64K random pairs on the current graph, device arrays
         n_r = 1 << 16
         rng = np.random.default_rng(77)

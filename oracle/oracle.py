@@ -104,6 +104,10 @@ def ref():
         R.ref_inc_dist.restype = None
         R.ref_reachable.restype = None
         R.ref_sssp.argtypes = [_P, ctypes.c_int32, ctypes.c_uint64, _P]
+        R.ref_bfs_two_level.argtypes = [_P, ctypes.c_int32, _P]
+        R.ref_bfs_two_level.restype = None
+        R.ref_sssp_two_level.argtypes = [_P, ctypes.c_int32, ctypes.c_uint64, _P]
+        R.ref_sssp_two_level.restype = None
         R.ref_edge_weight.argtypes = [ctypes.c_int32, ctypes.c_int32]
         R.ref_edge_weight.restype = ctypes.c_uint32
         R.ref_apply_batch.argtypes = [_P, _P, _P, _P, _I64]
@@ -451,6 +455,18 @@ class RefGIR:
     def sssp(self, s, delta=16):
         out = np.zeros(max(self.V, 1), np.uint64)
         ref().ref_sssp(self.h, s, delta, ptr(out))
+        return out[:self.V]
+
+    def bfs_two_level(self, s):
+        """GIR::bfsTwoLevel (the DAG wavefront; needs the layers built)."""
+        out = np.zeros(max(self.V, 1), np.int32)
+        ref().ref_bfs_two_level(self.h, s, ptr(out))
+        return out[:self.V]
+
+    def sssp_two_level(self, s, delta=16):
+        """GIR::ssspTwoLevel."""
+        out = np.zeros(max(self.V, 1), np.uint64)
+        ref().ref_sssp_two_level(self.h, s, delta, ptr(out))
         return out[:self.V]
 
     def apply_batch(self, u, v, ins):

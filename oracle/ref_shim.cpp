@@ -83,6 +83,18 @@ void ref_sssp(void* h, int32_t src, uint64_t delta, uint64_t* dist) {
     std::memcpy(dist, r.data(), sizeof(uint64_t) * r.size());
 }
 
+// GIR::bfsTwoLevel / ssspTwoLevel (gir_query.cpp:604-620, 705-722): the DAG wavefront with block
+// tasks inside the source SCC; same results as bfs / sssp.
+void ref_bfs_two_level(void* h, int32_t src, int32_t* level) {
+    auto r = static_cast<GIR*>(h)->bfsTwoLevel(src);
+    std::memcpy(level, r.data(), sizeof(int32_t) * r.size());
+}
+
+void ref_sssp_two_level(void* h, int32_t src, uint64_t delta, uint64_t* dist) {
+    auto r = static_cast<GIR*>(h)->ssspTwoLevel(src, delta);
+    std::memcpy(dist, r.data(), sizeof(uint64_t) * r.size());
+}
+
 uint32_t ref_edge_weight(int32_t u, int32_t v) { return GIR::edgeWeight(u, v); }
 
 void ref_apply_batch(void* h, const int32_t* u, const int32_t* v, const uint8_t* ins, int64_t n) {

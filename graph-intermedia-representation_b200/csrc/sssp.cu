@@ -33,9 +33,8 @@ constexpr uint64_t kInf = ~0ull;
 // [3] min live far distance, [4] far queue length after a split, [5] relaxation items,
 // [6] set when a 16-bit lane distance could not hold a tentative distance;
 // accumulated over the call: [16] reached (vertex, lane) pairs, [17] their out-edges
-// [7] the relaxation's item cursor, [8] (edge, lane) pairs of the pass (both cleared with [5]);
-enum { S_NEAR = 0, S_FAR = 1, S_SET = 2, S_MIN = 3, S_FAR2 = 4, S_ITEMS = 5, S_OVF = 6, S_CURSOR = 7, S_PAIRS = 8,
-       S_REACHED = 16, S_EDGES = 17, S_N = 32 };
+enum { S_NEAR = 0, S_FAR = 1, S_SET = 2, S_MIN = 3, S_FAR2 = 4, S_ITEMS = 5, S_OVF = 6, S_REACHED = 16, S_EDGES = 17,
+       S_N = 32 };
 
 // Sort keys (row << 32 | weight) and columns of every entry of the compact copy of `c`. For the
 // forward CSR the weight of entry (u, v) is that of edge u -> v. With `reverse` the rows are
@@ -179,14 +178,11 @@ struct Relax {
 // an exclusive scan of the items' work (edges x lanes) numbers all (edge, lane) pairs, and
 // k_relax processes them in equal runs, so a hub with many lanes is spread over the grid.
 struct Items {
-    int32_t* u;              // vertex
-    int32_t* ne;             // edges of the item (a run of the vertex's light or heavy edges)
-    int64_t* eb;             // first edge
-    unsigned long long* m;   // lanes
+    int32_t* u;
+    int64_t* eb;
+    unsigned long long* m;
+    int64_t* pref;  // work per item, then its exclusive scan (n + 1 entries)
 };
-// An item holds at most this many (edge, lane) pairs: a vertex with more work (a hub with many
-// lanes) is cut into several items, so no warp's window of 32 items can hold a whole hub.
-constexpr int64_t kItemPairs = 4096;
 
 // Number of light edges (weight < delta) of every weight-sorted row, once per query group.
 // Written with it, one 16-byte record per vertex for the queue bookkeeping of every pass: the
@@ -206,26 +202,18 @@ __global__ void k_light_split(int64_t V, const int64_t* wb, const int32_t* wdeg,
     }
 }
 
-// Takes every queued vertex's lanes (clearing them), does the settle bookkeeping and cuts the
-// vertex's work (its light edges, or with `heavy` its heavy edges, x its lanes) into items of at
-// most kItemPairs pairs. Each CTA reserves the slots of all its items with one atomicAdd on
-// cnt[S_ITEMS] and writes them cooperatively (a hub's items are spread over the CTA's threads);
-// cnt[S_PAIRS] gets the pass's pairs.
-__global__ void __launch_bounds__(kBlock) k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a,
-                                                       const int4* rows, Items it) {
+// Takes every queued vertex's lanes (clearing them), does the settle bookkeeping and appends an
+// item (vertex, first edge, lane mask, work = edges x lanes) for every vertex with work; the
+// item count goes to cnt[S_ITEMS]. Item slots past the count keep the zero work they were
+// cleared to, so a scan over all n + 1 slots needs no count from the host.
+__global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, const int4* rows, Items it) {
     __shared__ int s_w[kBlock / 32];
     __shared__ unsigned long long s_base;
-    __shared__ int32_t s_u[kBlock], s_ce[kBlock];
-    __shared__ int64_t s_eb[kBlock], s_e[kBlock];
-    __shared__ unsigned long long s_m[kBlock];
-    __shared__ int s_excl[kBlock + 1];
-    __shared__ int s_wsum[kBlock / 32];
-    __shared__ unsigned long long s_pairs;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
         int32_t u = 0;
         unsigned long long m = 0;
-        int64_t eb = 0, e = 0;
+        int64_t eb = 0, work = 0;
         bool settles = false;
         if (i < n) {
             u = q[i];
@@ -241,107 +229,78 @@ __global__ void __launch_bounds__(kBlock) k_relax_prep(const int32_t* q, int64_t
             const int64_t b = (int64_t)(((uint64_t)(uint32_t)r.y << 32) | (uint32_t)r.x);
             const int32_t nlu = r.w;
             eb = heavy ? b + nlu : b;
-            e = m ? (heavy ? r.z - nlu : nlu) : 0;
+            work = (int64_t)(heavy ? r.z - nlu : nlu) * __popcll(m);
         }
         const unsigned long long ss = block_slot(settles, &a.cnt[S_SET], s_w, &s_base);
         if (settles) a.setq[ss] = u;
-        // items of this thread's vertex: ce edges each (at most kItemPairs pairs)
-        const int pc = __popcll(m);
-        const int64_t ce = pc ? (kItemPairs / pc > 0 ? kItemPairs / pc : 1) : 1;
-        const int nch = e > 0 ? (int)((e + ce - 1) / ce) : 0;
-        // block exclusive scan of the item counts, one reservation for the CTA
-        int incl = nch;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if ((threadIdx.x & 31) >= o) incl += t;
+        const bool has = work > 0;
+        const unsigned long long slot = block_slot(has, &a.cnt[S_ITEMS], s_w, &s_base);
+        if (has) {
+            it.u[slot] = u;
+            it.eb[slot] = eb;
+            it.m[slot] = m;
+            it.pref[slot] = work;
         }
-        unsigned long long pairs = (unsigned long long)e * (unsigned long long)pc;
-        for (int o = 16; o; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
-        if ((threadIdx.x & 31) == 31) s_wsum[threadIdx.x >> 5] = incl;
-        if (threadIdx.x == 0) s_pairs = 0;
-        __syncthreads();
-        if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&s_pairs, pairs);
-        if (threadIdx.x == 0) {
-            int tot = 0;
-            for (int k = 0; k < kBlock / 32; ++k) {
-                const int c = s_wsum[k];
-                s_wsum[k] = tot;
-                tot += c;
-            }
-            s_excl[kBlock] = tot;
-            s_base = tot ? atomicAdd(&a.cnt[S_ITEMS], (unsigned long long)tot) : 0ull;
-        }
-        __syncthreads();
-        s_excl[threadIdx.x] = s_wsum[threadIdx.x >> 5] + incl - nch;
-        s_u[threadIdx.x] = u;
-        s_eb[threadIdx.x] = eb;
-        s_e[threadIdx.x] = e;
-        s_ce[threadIdx.x] = (int32_t)ce;
-        s_m[threadIdx.x] = m;
-        if (threadIdx.x == 0 && s_pairs) atomicAdd(&a.cnt[S_PAIRS], s_pairs);
-        __syncthreads();
-        const int tot = s_excl[kBlock];
-        const unsigned long long b0 = s_base;
-        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
-            int lo = 0, hi = kBlock - 1;  // the thread whose items hold k: largest t with excl[t] <= k
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_excl[mid] <= k) lo = mid; else hi = mid - 1;
-            }
-            const int c = k - s_excl[lo];
-            const int64_t ce_t = s_ce[lo], first = (int64_t)c * ce_t;
-            const int64_t left = s_e[lo] - first;
-            const unsigned long long slot = b0 + (unsigned long long)k;
-            it.u[slot] = s_u[lo];
-            it.ne[slot] = (int32_t)(left < ce_t ? left : ce_t);
-            it.eb[slot] = s_eb[lo] + first;
-            it.m[slot] = s_m[lo];
-        }
-        __syncthreads();  // (the shared arrays are rewritten by the next round)
     }
 }
 
 constexpr int kRelaxThreads = 256;
 constexpr int kPairs = 2;  // pairs in flight per thread (with 6 CTAs per SM: measured best)
 
-// Relaxation of the pass's items. Every warp takes the next 32 items from the cursor, scans their
-// work (edges x lanes) across its lanes, and walks the window's pairs 32 x kPairs at a time; a
-// pair finds its item by a binary search over the window's prefix through shuffles, so there is
-// no grid-wide scan, no shared memory beyond the staged appends and no block barrier. Pairs are
-// enumerated edge-major within an item: consecutive threads take consecutive lanes (in lane
-// order, which the caller arranges so that neighbouring lanes share sectors) of one edge.
+// Largest e in [lo, hi] with pref[e] <= key, for a strictly increasing pref with
+// pref[lo] <= key. One warp, 32 probes a round: the window shrinks 32-fold per dependent load.
+__device__ __forceinline__ int64_t warp_search(const int64_t* pref, int64_t lo, int64_t hi, int64_t key) {
+    const int ln = lane_id();
+    while (hi > lo) {
+        const int64_t step = (hi - lo + 31) / 32;
+        const int64_t p = lo + (int64_t)(ln + 1) * step;
+        const bool c = p <= hi && pref[p] <= key;
+        const int t = __popc(__ballot_sync(0xffffffffu, c));
+        if (t > 0) lo += (int64_t)t * step;
+        hi = lo + step - 1 < hi ? lo + step - 1 : hi;
+    }
+    return lo;
+}
+
+// Load-balanced relaxation over all (edge, lane) pairs of the item list, numbered by the
+// exclusive scan of the items' work. Every warp takes one contiguous run of pairs and finds the
+// item holding its first pair with one warp search. It then walks windows of 32 consecutive
+// items, one item per lane in registers: a pair finds its item by a binary search over the
+// window through shuffles, so no shared memory and no block barrier is involved and warps
+// proceed independently. Pairs are enumerated edge-major within an item: with many lanes
+// active, consecutive threads update consecutive lanes of one distance row.
 template <class D>
-__global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long long* cnt, unsigned long long* cursor,
-                                                            Items it, Relax a) {
+__global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long long* n_items, Items it, Relax a) {
     D* const dist = static_cast<D*>(a.dist);
-    const int64_t n = (int64_t)cnt[S_ITEMS];
+    const int64_t n = (int64_t)*n_items;
     if (n == 0) return;
+    const int64_t total = it.pref[n];
     __shared__ int32_t s_near[kRelaxThreads / 32][kStage], s_far[kRelaxThreads / 32][kStage];
     int n_near = 0, n_far = 0;
     const int ln = lane_id();
-    while (true) {
-        unsigned long long wb = 0;
-        if (ln == 0) wb = atomicAdd(cursor, 32ull);
-        wb = __shfl_sync(0xffffffffu, wb, 0);
-        if ((int64_t)wb >= n) break;
-        const int64_t ej = (int64_t)wb + ln;
-        int64_t ebj = 0, wj = 0;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t per = (((total + nw - 1) / nw) + 31) & ~(int64_t)31;
+    const int64_t c0 = gw * per;
+    const int64_t c1 = c0 + per < total ? c0 + per : total;
+    if (c0 >= c1) return;
+    int64_t e0 = warp_search(it.pref, 0, n - 1, c0);
+    int64_t p = c0;
+    while (p < c1) {
+        // window: items e0 .. e0+31, lane j holding item e0+j
+        const int64_t ej = e0 + ln;
+        int64_t pj = INT64_MAX, ebj = 0;
         unsigned long long mj = 0;
         int32_t uj = 0;
         if (ej < n) {
-            uj = it.u[ej];
+            pj = it.pref[ej];
             ebj = it.eb[ej];
             mj = it.m[ej];
-            wj = (int64_t)it.ne[ej] * __popcll(mj);
+            uj = it.u[ej];
         }
-        int64_t incl = wj;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (ln >= o) incl += t;
-        }
-        const int64_t pj = incl - wj;  // exclusive prefix: the window's first pair of item ej
-        const int64_t total = __shfl_sync(0xffffffffu, incl, 31);
-        for (int64_t p = 0; p < total; p += 32 * kPairs) {
+        const int64_t wnext = e0 + 32 < n ? it.pref[e0 + 32] : total;
+        const int64_t wend = wnext < c1 ? wnext : c1;
+        for (; p < wend; p += 32 * kPairs) {
             int32_t w[kPairs], sl[kPairs];
             int64_t k[kPairs];
             uint64_t du[kPairs];
@@ -349,8 +308,8 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
 #pragma unroll
             for (int j = 0; j < kPairs; ++j) {
                 const int64_t q = p + j * 32 + ln;
-                on[j] = q < total;
-                int x = 0;  // largest x with pj(x) <= q (items past n have pj = total)
+                on[j] = q < wend;
+                int x = 0;  // largest x with pref(x) <= q
 #pragma unroll
                 for (int b = 16; b; b >>= 1) {
                     const int64_t v = __shfl_sync(0xffffffffu, pj, x + b);
@@ -398,6 +357,8 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
                 stage_append(to_far, w[j], s_far[threadIdx.x >> 5], n_far, a.farq, &a.cnt[S_FAR]);
             }
         }
+        p = wend;  // (the pairs of this window end exactly where item e0+32 begins)
+        e0 += 32;
     }
     stage_flush(s_near[threadIdx.x >> 5], n_near, a.nextq, &a.cnt[S_NEAR]);
     stage_flush(s_far[threadIdx.x >> 5], n_far, a.farq, &a.cnt[S_FAR]);
@@ -586,12 +547,8 @@ struct Work {
     unsigned long long* hc;  // pinned host copy of the counters
 };
 
-// Item capacity: a queued vertex (at most once per pass) with e edges and pc lanes makes
-// ceil(e / floor(kItemPairs / pc)) <= 1 + e * pc / (kItemPairs - pc) items, and a pass's (edge,
-// lane) pairs are at most edges x 64, so V + 2 x edges x 64 / kItemPairs bounds every pass.
-int sssp_work(gir_dev* g, Work& w, int64_t E) {
+int sssp_work(gir_dev* g, Work& w) {
     const int64_t V = g->V;
-    const int64_t n_items = V + 2 * ((E * 64 + kItemPairs - 1) / kItemPairs) + 64;
     GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &w.nearq));
     GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &w.nextq));
     GIR_TRY(ensure_n(g, g->scratch[2], V + 1, &w.farq));
@@ -603,10 +560,10 @@ int sssp_work(gir_dev* g, Work& w, int64_t E) {
     GIR_TRY(ensure_n(g, g->scratch[12], V + 1, &w.setmask));
     GIR_TRY(ensure_n(g, g->scratch[13], S_N, &w.cnt));
     GIR_TRY(ensure_n(g, g->qitems[3], V + 1, &w.rows));
-    GIR_TRY(ensure_n(g, g->qitems[0], n_items, &w.items.u));
-    GIR_TRY(ensure_n(g, g->qitems[1], n_items, &w.items.eb));
-    GIR_TRY(ensure_n(g, g->qitems[2], n_items, &w.items.m));
-    GIR_TRY(ensure_n(g, g->qitems[4], n_items, &w.items.ne));
+    GIR_TRY(ensure_n(g, g->qitems[0], V + 1, &w.items.u));
+    GIR_TRY(ensure_n(g, g->qitems[1], V + 1, &w.items.eb));
+    GIR_TRY(ensure_n(g, g->qitems[2], V + 1, &w.items.m));
+    GIR_TRY(ensure_n(g, g->qitems[4], V + 2, &w.items.pref));
     void* h = nullptr;
     GIR_TRY(pinned(g, 256, &h));
     w.hc = static_cast<unsigned long long*>(h);
@@ -671,25 +628,25 @@ int sssp_group(gir_dev* g, Work& wk, const DevCSR& ws, int nl, const int64_t* la
     GIR_LAUNCH(g, "k_light_split");
     Items items = wk.items;
     // one relaxation pass over queue q (n entries): prep, scan of the work, balanced run
-    // items, cursor and pair count of a pass (cnt[S_ITEMS .. S_PAIRS]) are cleared together
-    static_assert(S_CURSOR == S_ITEMS + 2 && S_PAIRS == S_ITEMS + 3, "counter layout");
     auto relax = [&](const int32_t* q, int64_t n, int heavy) -> int {
-        GIR_CUDA(g, cudaMemsetAsync(cnt + S_ITEMS, 0, sizeof(unsigned long long) * 4, g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(cnt + S_ITEMS, 0, sizeof(unsigned long long), g->stream));
+        GIR_CUDA(g, cudaMemsetAsync(items.pref, 0, sizeof(int64_t) * (n + 1), g->stream));
         k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, wk.rows, items);
         GIR_LAUNCH(g, "k_relax_prep");
+        GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));
+        if (g->trace_marks) {
+            int64_t tot = 0;
+            GIR_CUDA(g, cudaMemcpyAsync(&tot, items.pref + n, sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
+            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
+            trace_pairs += tot;
+            ++trace_passes;
+        }
         GIR_TRY(timer.run([&]() -> int {
-            k_relax<D><<<run_grid, kRelaxThreads, 0, g->stream>>>(cnt, cnt + S_CURSOR, items, a);
+            k_relax<D><<<run_grid, kRelaxThreads, 0, g->stream>>>(cnt + S_ITEMS, items, a);
             GIR_LAUNCH(g, "k_relax");
             return GIR_OK;
         }));
-        if (g->trace_marks) {
-            unsigned long long tot = 0;
-            GIR_CUDA(g, cudaMemcpyAsync(&tot, cnt + S_PAIRS, sizeof(tot), cudaMemcpyDeviceToHost, g->stream));
-            GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-            trace_pairs += (int64_t)tot;
-            ++trace_passes;
-        }
-        st.launches += 2;  // prep and the relaxation
+        st.launches += 4;  // prep, the scan's two kernels, the relaxation
         return GIR_OK;
     };
     while (true) {
@@ -777,7 +734,7 @@ static int hub_order(gir_dev* g, int hash) {
     DevCSR wsb;
     int rc = build_weight_sorted(g, hash, 1, wsb);
     Work wk;
-    if (!rc) rc = sssp_work(g, wk, wsb.E);
+    if (!rc) rc = sssp_work(g, wk);
     int64_t* lanes = nullptr;
     if (!rc) rc = ensure_n(g, g->sssp_lanes, 4, &lanes);
     unsigned long long st[2] = {0, 0};
@@ -854,7 +811,7 @@ int sssp_run(gir_dev* g, const int64_t* set_beg_h, const int32_t* srcs_d, int64_
         std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return key[x] < key[y]; });
     }
     Work wk;
-    GIR_TRY(sssp_work(g, wk, ws.E));
+    GIR_TRY(sssp_work(g, wk));
     int64_t* lanes = nullptr;  // lane ranges (2 per lane), then output rows (1 per lane)
     GIR_TRY(ensure_n(g, g->sssp_lanes, 3 * 64, &lanes));
     // Lane distance width (GIR_PARAM_LANE_BITS): by default 32 bits when every finite distance

@@ -288,8 +288,6 @@ int select_flagged_i32(gir_dev* g, const int32_t* in, const uint8_t* flags, int3
 int select_flagged_iota(gir_dev* g, const uint8_t* flags, int32_t* out, int64_t n, int64_t* host_n);
 
 // ---- layers ----
-// Components of the undirected view of a forward CSR; label = smallest vertex id (wcc.cu).
-int wcc_labels(gir_dev* g, const DevCSR& c, int32_t* label, int64_t* n_comp);
 int wcc_build(gir_dev* g);
 int wcc_union_pairs(gir_dev* g, const uint64_t* keys, int64_t n);
 int scc_build(gir_dev* g);

@@ -343,6 +343,7 @@ int bct_build(gir_dev* g) {
         GIR_CUDA(g, cudaStreamSynchronize(g->stream));
         return GIR_OK;
     };
+    trace_mark(g, "bct: start");
     // 1. BFS forest; order[] holds the levels back to back, lvl_off their boundaries
     GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 2 * C_N, g->stream));
     uint8_t* nontrivial = nullptr;
@@ -374,6 +375,7 @@ int bct_build(gir_dev* g) {
         lvl_off.push_back(lvl_off.back() + (int64_t)hc[C_Q]);
     }
     const int D = (int)lvl_off.size() - 1;  // levels 0..D-1 (the last entry repeats the end)
+    trace_mark(g, "bct: forest");
     // 2. subtree sizes, bottom-up
     k_fill_i32<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(nd, V, 1);
     GIR_LAUNCH(g, "k_fill_i32");
@@ -406,6 +408,7 @@ int bct_build(gir_dev* g) {
         k_pre_level<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(order + lvl_off[L], n, parent, off, pre);
         GIR_LAUNCH(g, "k_pre_level");
     }
+    trace_mark(g, "bct: subtree sizes + preorder");
     // 3. low / high and rule 1
     GIR_CUDA(g, cudaMemcpyAsync(low, pre, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, g->stream));
     GIR_CUDA(g, cudaMemcpyAsync(high, pre, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, g->stream));
@@ -423,9 +426,11 @@ int bct_build(gir_dev* g) {
         k_lowhigh_level<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(order + lvl_off[L], n, parent, low, high);
         GIR_LAUNCH(g, "k_lowhigh_level");
     }
+    trace_mark(g, "bct: low/high + rule 1");
     // 4. rule 2
     k_rule2<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, parent, pre, nd, low, high, uf, &cnt[C_ERR]);
     GIR_LAUNCH(g, "k_rule2");
+    trace_mark(g, "bct: rule 2");
     // 5. blocks
     k_block_flags<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, parent, nd, uf, flag);
     GIR_LAUNCH(g, "k_block_flags");
@@ -448,6 +453,7 @@ int bct_build(gir_dev* g) {
     if (hc[C_ERR]) return fail(g, GIR_ERR_TIMEOUT, "bct: union-find exceeded its retry bound");
     g->n_blocks = nb;
     g->bct_built = true;
+    trace_mark(g, "bct: blocks");
     return GIR_OK;
 }
 

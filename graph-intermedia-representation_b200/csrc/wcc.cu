@@ -176,6 +176,7 @@ static int wcc_labels_sym(gir_dev* g, int32_t* label, int64_t* n_comp) {
         if (j - i > best) { best = j - i; giant = hs[i]; }
         i = j;
     }
+    trace_mark(g, "wcc: neighbour rounds + sample");
     k_uf_link_rest<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(s, V, kNeighbourRounds, giant, label, err);
     GIR_LAUNCH(g, "k_uf_link_rest");
     k_uf_compress<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(label, V, roots);

@@ -186,6 +186,7 @@ static int wcc_labels_sym(gir_dev* g, int32_t* label, int64_t* n_comp) {
     GIR_CUDA(g, cudaStreamSynchronize(g->stream));
     if (h[1]) return fail(g, GIR_ERR_TIMEOUT, "wcc: union-find link exceeded its retry bound");
     *n_comp = (int64_t)h[0];
+    trace_mark(g, "wcc: rest + compress");
     return GIR_OK;
 }
 

@@ -548,9 +548,11 @@ def ev_time(stream, fn):
     return e0.elapsed_time(e1)
 
 
-def compare_schedules(pkg, d, stream, sb, ss, lv, ds, weights, delta_fixed, reps):
+def compare_schedules(pkg, d, stream, sb, ss, lv, ds, weights, delta_fixed, reps, mean_weight=None):
     """The same BFS and SSSP sources under the fixed heuristics (the reference's alpha/beta switch
-    and delta) and under the trained schedule network; results must be identical."""
+    and delta) and under the trained schedule network; results must be identical. With
+    mean_weight, SSSP also runs with a one-line weight rule (delta = the candidate nearest, in log
+    scale, to the mean edge weight) as a second baseline for the network's delta."""
     import torch
     native = pkg.native
     out = {}
@@ -574,6 +576,15 @@ def compare_schedules(pkg, d, stream, sb, ss, lv, ds, weights, delta_fixed, reps
                    "fixed_delta": delta_fixed,
                    "learned_delta": [int(choices[c - 2]) for c in y_sssp.tolist() if c >= 2]}
     out["both_speedup"] = (t_bf + t_sf) / (t_bl + t_sl)
+    if mean_weight:
+        import math
+        rule = int(min(choices, key=lambda c: abs(math.log2(c) - math.log2(mean_weight))))
+        ds3 = torch.empty_like(ds)
+        d.sssp(ss, delta=rule, weights=weights, out=ds3)
+        t_sr = min(ev_time(stream, lambda: d.sssp(ss, delta=rule, weights=weights, out=ds3)) for _ in range(reps))
+        out["sssp"]["weight_rule"] = {"delta": rule, "ms": t_sr, "speedup_vs_fixed": t_sf / t_sr,
+                                      "learned_vs_rule": t_sr / t_sl, "identical": bool(torch.equal(ds, ds3)),
+                                      "mean_weight": mean_weight}
     return out
 
 
@@ -794,7 +805,8 @@ def run_ours(args):
 
     # learned vs fixed schedule on this graph (same sources, identical results required)
     if not args.no_schedule:
-        sch = {args.workload: compare_schedules(pkg, d, stream, sb_d, ss_d, lv_d, ds_d, native.WEIGHT_HASH, DELTA, 2)}
+        sch = {args.workload: compare_schedules(pkg, d, stream, sb_d, ss_d, lv_d, ds_d, native.WEIGHT_HASH, DELTA, 2,
+                                                mean_weight=50.5)}  # (GIR::edgeWeight is uniform on [1, 100])
 
     # layer builds and update batches (every layer kept exact)
     upd = {}
@@ -892,7 +904,8 @@ def run_ours(args):
         sl_s = torch.from_numpy(pkg.graphs.sources_with_edges(gl, N_SSSP, 22 + 1000 * rank)).to(dev)
         lv_l = torch.empty((N_BFS, gl.V), dtype=torch.int32, device=dev)
         ds_l = torch.empty((N_SSSP, gl.V), dtype=torch.int64, device=dev)
-        res = compare_schedules(pkg, d, stream, sl_b, sl_s, lv_l, ds_l, native.WEIGHT_STORED, DELTA, 1)
+        res = compare_schedules(pkg, d, stream, sl_b, sl_s, lv_l, ds_l, native.WEIGHT_STORED, DELTA, 1,
+                                mean_weight=float(np.mean(gl.w)))
         res["build_wcc_scc_bct_ms"] = ev_time(stream, lambda: d.build(native.LAYER_ALL))
         res["graph"] = f"lattice 4900 x 4900, 5% removed, 0.1% Pareto(1.5) long-range, V={gl.V}, E={gl.E}"
         sch["lattice"] = res

@@ -819,7 +819,7 @@ int gir_dev_destroy(gir_dev_t* g) {
         store_free(g, g->ws[0]); store_free(g, g->ws[1]);
         for (DevBuf* b : {&g->wcc, &g->scc, &g->scc_rank, &g->dag, &g->dag_rows, &g->reach_hub, &g->blk_label, &g->blk_head, &g->bcnt, &g->bins,
                           &g->cub_tmp, &g->stage_in, &g->stage_out, &g->sched_w, &g->sched_io, &g->lane_dist, &g->inc_st[0], &g->inc_st[1],
-                          &g->inc_pend[0], &g->inc_pend[1], &g->single_ws, &g->hub_dist[0], &g->hub_dist[1], &g->sssp_sets, &g->sssp_lanes, &g->pend_pairs})
+                          &g->inc_pend[0], &g->inc_pend[1], &g->single_ws, &g->hub_dist[0], &g->hub_dist[1], &g->sssp_sets, &g->sssp_lanes, &g->sssp_done, &g->pend_pairs})
             release(g, *b);
         for (auto& b : g->scratch) release(g, b);
         for (auto& b : g->work) release(g, b);

@@ -150,6 +150,7 @@ struct gir_dev {
     gir::DevBuf qitems[5];            // per-queue-entry work items of the SSSP relaxation
     gir::DevBuf sssp_sets;            // SSSP: every set's source range and lane-order key
     gir::DevBuf sssp_lanes;           // SSSP: one lane group's source ranges and output rows
+    gir::DevBuf sssp_done;            // SSSP: per vertex, the lanes whose distance is final
     void* pinned = nullptr;           // small pinned host buffer for counters
     size_t pinned_bytes = 0;
 

@@ -207,10 +207,12 @@ __global__ void k_light_split(int64_t V, const int64_t* wb, const int32_t* wdeg,
     }
 }
 
-// Takes every queued vertex's lanes (clearing them), does the settle bookkeeping and appends an
-// item (vertex, first edge, lane mask, work = edges x lanes) for every vertex with work; the
-// item count goes to cnt[S_ITEMS]. Item slots past the count keep the zero work they were
-// cleared to, so a scan over all n + 1 slots needs no count from the host.
+// Takes every queued vertex's lanes (clearing them), does the settle bookkeeping and writes queue
+// entry i's item (vertex, first edge, lane mask, work = edges x lanes) into slot i; cnt[S_ITEMS]
+// = n and pref[n] = 0, so the scan of the n + 1 slots needs nothing cleared beforehand. Items
+// without work stay in place: the relaxation's searches take the largest item whose prefix is at
+// most the pair's index, which is never a zero-work item (its prefix equals the next item's).
+// A vertex is queued once per pass, so its setmask word is touched by one thread only.
 __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, const int4* rows, Items it) {
     __shared__ int s_w[kBlock / 32];
     __shared__ unsigned long long s_base;
@@ -229,32 +231,35 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
             } else {
                 m = a.curmask[u];
                 a.curmask[u] = 0ull;
-                settles = m && atomicOr(&a.setmask[u], m) == 0ull;
+                const unsigned long long old = a.setmask[u];
+                a.setmask[u] = old | m;
+                settles = m && old == 0ull;
             }
             const int4 r = rows[u];
             const int64_t b = (int64_t)(((uint64_t)(uint32_t)r.y << 32) | (uint32_t)r.x);
             const int32_t nlu = r.w;
             eb = heavy ? b + nlu : b;
             work = (int64_t)(heavy ? r.z - nlu : nlu) * __popcll(m);
+            it.u[i] = u;
+            it.eb[i] = eb;
+            it.m[i] = m;
+            it.pref[i] = work;
         }
         const unsigned long long ss = block_slot(settles, &a.cnt[S_SET], s_w, &s_base);
         if (settles) a.setq[ss] = u;
-        const bool has = work > 0;
-        const unsigned long long slot = block_slot(has, &a.cnt[S_ITEMS], s_w, &s_base);
-        if (has) {
-            it.u[slot] = u;
-            it.eb[slot] = eb;
-            it.m[slot] = m;
-            it.pref[slot] = work;
-        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        it.pref[n] = 0;
+        a.cnt[S_ITEMS] = (unsigned long long)n;
     }
 }
 
 constexpr int kRelaxThreads = 256;
 constexpr int kPairs = 2;  // pairs in flight per thread (with 6 CTAs per SM: measured best)
 
-// Largest e in [lo, hi] with pref[e] <= key, for a strictly increasing pref with
-// pref[lo] <= key. One warp, 32 probes a round: the window shrinks 32-fold per dependent load.
+// Largest e in [lo, hi] with pref[e] <= key, for a non-decreasing pref with pref[lo] <= key
+// (the probes at or below the key are a prefix of each round's 32). One warp, 32 probes a round:
+// the window shrinks 32-fold per dependent load.
 __device__ __forceinline__ int64_t warp_search(const int64_t* pref, int64_t lo, int64_t hi, int64_t key) {
     const int ln = lane_id();
     while (hi > lo) {
@@ -640,8 +645,6 @@ int sssp_group(gir_dev* g, Work& wk, const DevCSR& ws, int nl, const int64_t* la
     Items items = wk.items;
     // one relaxation pass over queue q (n entries): prep, scan of the work, balanced run
     auto relax = [&](const int32_t* q, int64_t n, int heavy) -> int {
-        GIR_CUDA(g, cudaMemsetAsync(cnt + S_ITEMS, 0, sizeof(unsigned long long), g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(items.pref, 0, sizeof(int64_t) * (n + 1), g->stream));
         k_relax_prep<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(q, n, heavy, a, wk.rows, items);
         GIR_LAUNCH(g, "k_relax_prep");
         GIR_TRY(exclusive_scan_i64(g, items.pref, items.pref, n + 1));

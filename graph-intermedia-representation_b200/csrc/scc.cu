@@ -291,44 +291,6 @@ __global__ void __launch_bounds__(kBlock) k_cross_keys(int64_t V, CSRView fw, co
     });
 }
 
-// Condensation keys deduplicated in an open-addressing hash table (`cap` slots, a power of two,
-// all ~0 = empty) before anything is sorted: each distinct (label(u), label(v)) key of an edge
-// between two SCCs is appended once to `out` (count cnt[0]). A warp's lanes with the same key
-// (consecutive edges of one row into one SCC) probe once. cnt[1] is set when the table holds
-// more than half its slots or a probe runs past its bound: the caller then falls back to sorting
-// every cross key.
-__global__ void __launch_bounds__(kBlock) k_cross_hash(int64_t V, CSRView fw, const int32_t* label, uint64_t* table,
-                                                       uint64_t cap, uint64_t* out, unsigned long long* cnt) {
-    __shared__ int64_t s_excl[kWarps][33];
-    __shared__ int32_t s_u[kWarps][32];
-    const int wib = threadIdx.x >> 5;
-    const uint64_t mask = cap - 1;
-    warp_sweep_rows(fw.beg, fw.deg, fw.adj, 0, V, s_excl[wib], s_u[wib], [&](int32_t u, int32_t w, int64_t) {
-        const int32_t a = label[u], b = label[w];
-        if (a == b) return;
-        const uint64_t key = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
-        const unsigned grp = __match_any_sync(__activemask(), key);
-        if ((int)(__ffs(grp) - 1) != lane_id()) return;
-        uint64_t h = key * 0x9e3779b97f4a7c15ULL;
-        h ^= h >> 29;
-        for (uint64_t probe = 0; probe < 4096; ++probe, h = (h + 1) & mask) {
-            const uint64_t slot = h & mask;
-            const uint64_t cur = *(volatile uint64_t*)&table[slot];
-            if (cur == key) return;
-            if (cur != ~0ull) continue;
-            const uint64_t prev = atomicCAS((unsigned long long*)&table[slot], ~0ull, (unsigned long long)key);
-            if (prev == ~0ull) {
-                const unsigned long long k = atomicAdd(&cnt[0], 1ull);
-                if (k < cap / 2) out[k] = key;
-                else cnt[1] = 1ull;
-                return;
-            }
-            if (prev == key) return;
-        }
-        cnt[1] = 1ull;  // (a probe run this long means the table is far too full)
-    });
-}
-
 __global__ void k_distinct_u64(const uint64_t* keys, int64_t n, uint8_t* flag) {
     GRID_STRIDE(i, n) flag[i] = (i == 0 || keys[i] != keys[i - 1]);
 }
@@ -678,49 +640,22 @@ int scc_build_dag(gir_dev* g) {
     void* hp = nullptr;
     GIR_TRY(pinned(g, 256, &hp));
     unsigned long long* hc = static_cast<unsigned long long*>(hp);
+    GIR_CUDA(g, cudaMemsetAsync(flag, 0, cap + 1, g->stream));
+    if (V > 0) {
+        k_cross_keys<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, view(g->fw), label, keys, flag);
+        GIR_LAUNCH(g, "k_cross_keys");
+    }
+    int64_t n_cross = 0;
+    GIR_TRY(select_flagged_u64(g, keys, flag, tmp, cap, &n_cross));
+    std::swap(keys, tmp);
+    GIR_TRY(sort_keys_u64(g, keys, tmp, n_cross, 64));
     int64_t n_dag = 0;
     uint64_t* dag = nullptr;
-    bool hashed = false;
-    if (V > 0) {
-        // distinct keys through a hash table sized from the last condensation (4x its keys, at
-        // least 2^20 slots, at most twice the vertices or the edge capacity)
-        uint64_t slots = 1u << 20;
-        const int64_t want = g->n_dag > 0 ? 4 * g->n_dag : 2 * V;
-        const int64_t top = 2 * V < cap ? 2 * V : cap;
-        while ((int64_t)slots < want && (int64_t)slots < top) slots <<= 1;
-        uint64_t* table = nullptr;
-        GIR_TRY(ensure_n(g, g->scratch[10], slots + 1, &table));
-        GIR_CUDA(g, cudaMemsetAsync(table, 0xff, sizeof(uint64_t) * slots, g->stream));
-        GIR_CUDA(g, cudaMemsetAsync(cnt + C_N, 0, sizeof(unsigned long long) * 2, g->stream));
-        k_cross_hash<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, view(g->fw), label, table, slots, keys,
-                                                                      cnt + C_N);
-        GIR_LAUNCH(g, "k_cross_hash");
-        GIR_CUDA(g, cudaMemcpyAsync(hc, cnt + C_N, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, g->stream));
-        GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-        if (!hc[1]) {
-            n_dag = (int64_t)hc[0];
-            GIR_TRY(ensure_n(g, g->dag, n_dag + 1, &dag));
-            GIR_TRY(sort_keys_u64(g, keys, tmp, n_dag, 64));
-            if (n_dag) GIR_CUDA(g, cudaMemcpyAsync(dag, keys, sizeof(uint64_t) * n_dag, cudaMemcpyDeviceToDevice, g->stream));
-            hashed = true;
-        }
-    }
-    if (!hashed) {  // every cross key, sorted, then unique
-        GIR_CUDA(g, cudaMemsetAsync(flag, 0, cap + 1, g->stream));
-        if (V > 0) {
-            k_cross_keys<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, view(g->fw), label, keys, flag);
-            GIR_LAUNCH(g, "k_cross_keys");
-        }
-        int64_t n_cross = 0;
-        GIR_TRY(select_flagged_u64(g, keys, flag, tmp, cap, &n_cross));
-        std::swap(keys, tmp);
-        GIR_TRY(sort_keys_u64(g, keys, tmp, n_cross, 64));
-        GIR_TRY(ensure_n(g, g->dag, n_cross + 1, &dag));
-        if (n_cross > 0) {
-            k_distinct_u64<<<grid_for(g, n_cross, kBlock), kBlock, 0, g->stream>>>(keys, n_cross, flag);
-            GIR_LAUNCH(g, "k_distinct_u64");
-            GIR_TRY(select_flagged_u64(g, keys, flag, dag, n_cross, &n_dag));
-        }
+    GIR_TRY(ensure_n(g, g->dag, n_cross + 1, &dag));
+    if (n_cross > 0) {
+        k_distinct_u64<<<grid_for(g, n_cross, kBlock), kBlock, 0, g->stream>>>(keys, n_cross, flag);
+        GIR_LAUNCH(g, "k_distinct_u64");
+        GIR_TRY(select_flagged_u64(g, keys, flag, dag, n_cross, &n_dag));
     }
     g->n_dag = n_dag;
     g->dag_rows_valid = false;

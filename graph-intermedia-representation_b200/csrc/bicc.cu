@@ -197,6 +197,40 @@ __global__ void k_pack_vinfo(int64_t V, const int32_t* pre, const int32_t* nd, c
     GRID_STRIDE(v, V) vinfo[v] = make_int4(pre[v], nd[v], parent[v], scc[v]);
 }
 
+// Rule-1 unions from a sample before the full sweep: every vertex of H takes the first kSample
+// entries of its row, and the non-tree edges among them whose ends are unrelated in the forest
+// (neither an ancestor of the other) union the two ends' tree edges. After a flatten (every uf
+// entry its root), the full sweep's cheap uf[u] != uf[w] test rejects nearly every pair the
+// sample already joined (on a power-law graph the giant block takes most vertices), instead of
+// each pair walking two find chains. Unions are idempotent, so the sample changes no class.
+constexpr int kSample = 4;
+
+__global__ void k_nontree_sample(int64_t V, HView h, const int4* vinfo, int32_t* uf, unsigned long long* err) {
+    GRID_STRIDE(u, V) {
+        const int32_t d = h.sym.deg[u];
+        if (d == 0) continue;
+        const int4 iu = vinfo[u];
+        const int64_t b = h.sym.beg[u];
+        for (int j = 0; j < kSample && j < d; ++j) {
+            const int32_t w = h.sym.adj[b + j];
+            const int4 iw = vinfo[w];
+            if (iu.w != iw.w || iw.z == (int32_t)u || iu.z == w) continue;  // other SCC, or a tree edge
+            const bool w_under_u = iw.x >= iu.x && iw.x < iu.x + iu.y;
+            const bool u_under_w = iu.x >= iw.x && iu.x < iw.x + iw.y;
+            if (!w_under_u && !u_under_w && uf[u] != uf[w]) uf_union(uf, (int32_t)u, w, err);
+        }
+    }
+}
+
+// Every uf entry to its root (read-only walks, then one write; no union runs meanwhile).
+__global__ void k_uf_flatten(int32_t* uf, int64_t V) {
+    GRID_STRIDE(v, V) {
+        int32_t x = uf[v];
+        while (uf[x] != x) x = uf[x];
+        uf[v] = x;
+    }
+}
+
 // One sweep over the non-tree edges of H: low / high of every vertex from its own non-tree
 // neighbours, and rule 1 (once per edge, from its endpoint with the smaller pre) for edges
 // between unrelated endpoints.
@@ -418,6 +452,10 @@ int bct_build(gir_dev* g) {
     GIR_TRY(ensure_n(g, g->work[5], V + 1, &vinfo));
     k_pack_vinfo<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, pre, nd, parent, scc, vinfo);
     GIR_LAUNCH(g, "k_pack_vinfo");
+    k_nontree_sample<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, h, vinfo, uf, &cnt[C_ERR]);
+    GIR_LAUNCH(g, "k_nontree_sample");
+    k_uf_flatten<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(uf, V);
+    GIR_LAUNCH(g, "k_uf_flatten");
     k_nontree<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, h, vinfo, low, high, uf, &cnt[C_ERR]);
     GIR_LAUNCH(g, "k_nontree");
     for (int L = D - 1; L >= 1; --L) {

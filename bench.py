@@ -199,12 +199,14 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch(kernel):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+def traffic_ratio(kernel):
+    """DRAM bytes over algorithmic bytes of the dominant kernel, measured by ncu on a smaller case of
+    the same kernel (the committed summary under profiles/), or None."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(kernel)
+            r = json.load(f).get(kernel)
+            return r.get("dram_over_algorithmic") if isinstance(r, dict) else None
     except (OSError, ValueError):
         return None
 
@@ -783,12 +785,14 @@ def run_ours(args):
         kern, kb, kms, kl = "BFS level kernels", bfs_bytes, qb["main_ms"], qb["main_launches"]
     peak, peak_src = measured_peak()
     achieved = kb / (kms * 1e-3) / 1e9
-    tr = traffic_per_launch(kern)
+    ratio = traffic_ratio(kern)
+    tr = ratio * kb / max(kl, 1) if ratio else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": tr, "kernel": kern, "launches": kl, "kernel_ms": kms,
                 "algorithmic_bytes": kb, "algorithmic_bytes_per_launch": kb / max(kl, 1),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, averaged over one "
-                                  "call (committed ncu summary under profiles/)" if tr else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of every launch of one 64-source "
+                                  "call on the 1M-vertex R-MAT (rmat_s20), as a ratio to that call's algorithmic "
+                                  "bytes, times this call's algorithmic bytes per launch" if tr else None,
                 "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"}
 
     # SSSP with the stored U[1,255] weights (the configuration's weights), reported beside

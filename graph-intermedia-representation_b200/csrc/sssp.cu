@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
 template <class D>
 __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar, unsigned long long* farmask,
                             const D* dist, int nl, uint64_t lo, uint64_t hi, unsigned long long* nearmask,
-                            int32_t* nearq, int32_t* farq2, unsigned long long* cnt) {
+                            int32_t* nearq, int32_t* farq2, const unsigned long long* done, unsigned long long* cnt) {
     const int64_t n = (int64_t)*nfar;
     __shared__ int32_t s_near[kBlock / 32][kStage], s_far[kBlock / 32][kStage];
     int n_near = 0, n_far = 0;
@@ -395,7 +395,8 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
         unsigned long long mn = kInf;
         if (i < n) {
             w = farq[i];
-            unsigned long long m = farmask[w], nm = 0, keep = 0;
+            // (lanes already final were reached by a shorter path since: dropped unread)
+            unsigned long long m = farmask[w] & ~done[w], nm = 0, keep = 0;
             while (m) {
                 const int s = __ffsll((long long)m) - 1;
                 m &= m - 1;
@@ -695,7 +696,7 @@ int sssp_group(gir_dev* g, Work& wk, const DevCSR& ws, int nl, const int64_t* la
             GIR_CUDA(g, cudaMemsetAsync(cnt + S_MIN, 0xff, sizeof(unsigned long long), g->stream));
             GIR_CUDA(g, cudaMemsetAsync(cnt + S_FAR2, 0, sizeof(unsigned long long), g->stream));
             k_far_split<D><<<grid_for(g, n_far, kBlock), kBlock, 0, g->stream>>>(
-                farq, cnt + S_FAR, wk.farmask, dist, nl, k * Dw, (k + 1) * Dw, curmask, nearq, farq2, cnt);
+                farq, cnt + S_FAR, wk.farmask, dist, nl, k * Dw, (k + 1) * Dw, curmask, nearq, farq2, wk.done, cnt);
             GIR_LAUNCH(g, "k_far_split");
             st.launches++;
             std::swap(farq, farq2);

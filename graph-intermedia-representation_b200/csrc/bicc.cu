@@ -234,19 +234,32 @@ __global__ void k_uf_flatten(int32_t* uf, int64_t V) {
 // One sweep over the non-tree edges of H: low / high of every vertex from its own non-tree
 // neighbours, and rule 1 (once per edge, from its endpoint with the smaller pre) for edges
 // between unrelated endpoints.
+__device__ __forceinline__ void nontree_entry(int32_t u, int32_t w, const int4* vinfo, int32_t* low, int32_t* high,
+                                              int32_t* uf, unsigned long long* err) {
+    const int4 iu = vinfo[u], iw = vinfo[w];
+    if (iu.w != iw.w || iw.z == u || iu.z == w) return;  // other SCC, or a tree edge
+    const int32_t pw = iw.x;
+    if (pw < low[u]) atomicMin(&low[u], pw);  // (plain pre-checks: a hub's row is swept by many
+    if (pw > high[u]) atomicMax(&high[u], pw);  //  threads, most of which change nothing)
+    if (iu.x < pw && iu.x + iu.y <= pw && uf[u] != uf[w]) uf_union(uf, u, w, err);
+}
+
+// Rows of at most kHeavyRow entries, a warp per 32 rows; the longer rows go to k_nontree_heavy,
+// which spreads their entries over the whole grid.
 __global__ void __launch_bounds__(kBlock) k_nontree(int64_t V, HView h, const int4* vinfo, int32_t* low, int32_t* high,
                                                     int32_t* uf, unsigned long long* err) {
     __shared__ int64_t s_excl[kBlock / 32][33];
     __shared__ int32_t s_u[kBlock / 32][32];
     const int wib = threadIdx.x >> 5;
-    warp_sweep_rows(h.sym.beg, h.sym.deg, h.sym.adj, 0, V, s_excl[wib], s_u[wib], [&](int32_t u, int32_t w, int64_t) {
-        const int4 iu = vinfo[u], iw = vinfo[w];
-        if (iu.w != iw.w || iw.z == u || iu.z == w) return;  // other SCC, or a tree edge
-        const int32_t pw = iw.x;
-        if (pw < low[u]) atomicMin(&low[u], pw);  // (plain pre-checks: a hub's row is swept by many
-        if (pw > high[u]) atomicMax(&high[u], pw);  //  threads, most of which change nothing)
-        if (iu.x < pw && iu.x + iu.y <= pw && uf[u] != uf[w]) uf_union(uf, u, w, err);
-    });
+    warp_sweep_rows(
+        h.sym.beg, h.sym.deg, h.sym.adj, 0, V, s_excl[wib], s_u[wib],
+        [&](int32_t u, int32_t w, int64_t) { nontree_entry(u, w, vinfo, low, high, uf, err); }, kHeavyRow);
+}
+
+__global__ void k_nontree_heavy(const int32_t* rows, const int64_t* pref, int64_t n, HView h, const int4* vinfo,
+                                int32_t* low, int32_t* high, int32_t* uf, unsigned long long* err) {
+    grid_sweep_heavy_rows(rows, pref, n, h.sym.beg, h.sym.adj,
+                          [&](int32_t u, int32_t w, int64_t) { nontree_entry(u, w, vinfo, low, high, uf, err); });
 }
 
 __global__ void k_lowhigh_level(const int32_t* q, int64_t n, const int32_t* parent, int32_t* low, int32_t* high) {
@@ -458,6 +471,16 @@ int bct_build(gir_dev* g) {
     GIR_LAUNCH(g, "k_uf_flatten");
     k_nontree<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, h, vinfo, low, high, uf, &cnt[C_ERR]);
     GIR_LAUNCH(g, "k_nontree");
+    {
+        int64_t n_heavy = 0;  // (first / scan are free after the preorder)
+        int32_t* heavy = reinterpret_cast<int32_t*>(first);
+        GIR_TRY(heavy_rows(g, h.sym.deg, V, kHeavyRow, flag, heavy, scan, &n_heavy));
+        if (n_heavy > 0) {
+            k_nontree_heavy<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(heavy, scan, n_heavy, h, vinfo, low, high,
+                                                                             uf, &cnt[C_ERR]);
+            GIR_LAUNCH(g, "k_nontree_heavy");
+        }
+    }
     for (int L = D - 1; L >= 1; --L) {
         const int64_t n = lvl_off[L + 1] - lvl_off[L];
         if (n == 0) continue;

@@ -287,6 +287,11 @@ int select_flagged_u64(gir_dev* g, const uint64_t* in, const uint8_t* flags, uin
 int select_flagged_i32(gir_dev* g, const int32_t* in, const uint8_t* flags, int32_t* out, int64_t n, int64_t* host_n);
 // Indices i in [0, n) with flags[i] != 0, ascending.
 int select_flagged_iota(gir_dev* g, const uint8_t* flags, int32_t* out, int64_t n, int64_t* host_n);
+// The rows of `deg` (V entries) longer than max_deg, ascending, into rows (V entries), and the
+// exclusive scan of their lengths into pref (V + 1 entries); *n = their number. flag: V bytes.
+constexpr int32_t kHeavyRow = 4096;
+int heavy_rows(gir_dev* g, const int32_t* deg, int64_t V, int32_t max_deg, uint8_t* flag, int32_t* rows, int64_t* pref,
+               int64_t* n);
 
 // ---- layers ----
 int wcc_build(gir_dev* g);
@@ -374,15 +379,20 @@ __device__ __forceinline__ int64_t lower_bound_dev(const T* a, int64_t lo, int64
 // so a row of any length costs its warp ceil(len/32) rounds. Must be called by all threads of
 // the grid (every lane of a warp takes part in every round). `scan` is per-warp shared scratch
 // of 33 int64 and 32 int32.
+// With max_deg >= 0, rows longer than max_deg are left out: a warp walks all of its 32 rows, so a
+// hub row would keep one warp busy long after the rest of the grid is idle; sweep those rows with
+// grid_sweep_heavy_rows instead (rows and offsets from heavy_rows).
 template <class F>
 __device__ __forceinline__ void warp_sweep_rows(const int64_t* beg, const int32_t* deg, const int32_t* adj,
-                                                int64_t v0, int64_t v1, int64_t* s_excl, int32_t* s_u, F&& f) {
+                                                int64_t v0, int64_t v1, int64_t* s_excl, int32_t* s_u, F&& f,
+                                                int32_t max_deg = -1) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t base = v0 + warp * 32; base < v1; base += nwarps * 32) {
         const int64_t v = base + lane;
-        const int64_t cnt = v < v1 ? deg[v] : 0;
+        int64_t cnt = v < v1 ? deg[v] : 0;
+        if (max_deg >= 0 && cnt > max_deg) cnt = 0;
         int64_t incl = cnt;
         for (int o = 1; o < 32; o <<= 1) {
             const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
@@ -407,6 +417,26 @@ __device__ __forceinline__ void warp_sweep_rows(const int64_t* beg, const int32_
             }
         }
         __syncwarp();
+    }
+}
+
+// Calls f(u, w, edge_index) for every entry of the rows rows[0 .. n) (pref: the exclusive scan of
+// their lengths, n + 1 entries), the entries spread evenly over the whole grid: the companion of
+// warp_sweep_rows(..., max_deg) for the rows it leaves out.
+template <class F>
+__device__ __forceinline__ void grid_sweep_heavy_rows(const int32_t* rows, const int64_t* pref, int64_t n,
+                                                      const int64_t* beg, const int32_t* adj, F&& f) {
+    if (n <= 0) return;
+    const int64_t total = pref[n];
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t lo = 0, hi = n - 1;  // largest r with pref[r] <= e
+        while (lo < hi) {
+            const int64_t m = (lo + hi + 1) >> 1;
+            if (pref[m] <= e) lo = m; else hi = m - 1;
+        }
+        const int32_t u = rows[lo];
+        const int64_t k = beg[u] + (e - pref[lo]);
+        f(u, adj[k], k);
     }
 }
 

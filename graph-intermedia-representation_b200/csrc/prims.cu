@@ -208,4 +208,28 @@ int select_flagged_iota(gir_dev* g, const uint8_t* flags, int32_t* out, int64_t 
     return select_flagged(g, cub::CountingInputIterator<int32_t>(0), flags, out, n, host_n);
 }
 
+namespace {
+__global__ void k_heavy_flags(const int32_t* deg, int64_t V, int32_t max_deg, uint8_t* flag) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x)
+        flag[v] = deg[v] > max_deg;
+}
+__global__ void k_heavy_lengths(const int32_t* deg, const int32_t* rows, int64_t n, int64_t* pref) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        pref[i] = deg[rows[i]];
+    if (blockIdx.x == 0 && threadIdx.x == 0) pref[n] = 0;
+}
+}  // namespace
+
+int heavy_rows(gir_dev* g, const int32_t* deg, int64_t V, int32_t max_deg, uint8_t* flag, int32_t* rows, int64_t* pref,
+               int64_t* n) {
+    *n = 0;
+    if (V <= 0) return GIR_OK;
+    k_heavy_flags<<<grid_for(g, V, 256), 256, 0, g->stream>>>(deg, V, max_deg, flag);
+    GIR_LAUNCH(g, "k_heavy_flags");
+    GIR_TRY(select_flagged_iota(g, flag, rows, V, n));
+    k_heavy_lengths<<<grid_for(g, *n + 1, 256), 256, 0, g->stream>>>(deg, rows, *n, pref);
+    GIR_LAUNCH(g, "k_heavy_lengths");
+    return exclusive_scan_i64(g, pref, pref, *n + 1);
+}
+
 }  // namespace gir

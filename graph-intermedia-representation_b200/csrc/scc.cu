@@ -284,7 +284,20 @@ __global__ void __launch_bounds__(kBlock) k_cross_keys(int64_t V, CSRView fw, co
     __shared__ int64_t s_excl[kWarps][33];
     __shared__ int32_t s_u[kWarps][32];
     const int wib = threadIdx.x >> 5;
-    warp_sweep_rows(fw.beg, fw.deg, fw.adj, 0, V, s_excl[wib], s_u[wib], [&](int32_t u, int32_t w, int64_t e) {
+    warp_sweep_rows(
+        fw.beg, fw.deg, fw.adj, 0, V, s_excl[wib], s_u[wib],
+        [&](int32_t u, int32_t w, int64_t e) {
+            const int32_t a = label[u], b = label[w];
+            keys[e] = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
+            flag[e] = a != b;
+        },
+        kHeavyRow);
+}
+
+// The rows k_cross_keys leaves out (longer than kHeavyRow), their entries spread over the grid.
+__global__ void k_cross_keys_heavy(const int32_t* rows, const int64_t* pref, int64_t n, CSRView fw, const int32_t* label,
+                                   uint64_t* keys, uint8_t* flag) {
+    grid_sweep_heavy_rows(rows, pref, n, fw.beg, fw.adj, [&](int32_t u, int32_t w, int64_t e) {
         const int32_t a = label[u], b = label[w];
         keys[e] = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
         flag[e] = a != b;
@@ -642,8 +655,20 @@ int scc_build_dag(gir_dev* g) {
     unsigned long long* hc = static_cast<unsigned long long*>(hp);
     GIR_CUDA(g, cudaMemsetAsync(flag, 0, cap + 1, g->stream));
     if (V > 0) {
+        // the long rows' list in tmp (free until the compaction; cap >= 4V, every row has room
+        // for 4 entries): rows int32[V], their length scan int64[V + 1], flags uint8[V]
+        int32_t* heavy = reinterpret_cast<int32_t*>(tmp);
+        int64_t* hpref = reinterpret_cast<int64_t*>(tmp) + (V + 1) / 2 + 1;
+        uint8_t* hflag = reinterpret_cast<uint8_t*>(hpref + V + 2);
+        int64_t n_heavy = 0;
+        GIR_TRY(heavy_rows(g, g->fw.deg, V, kHeavyRow, hflag, heavy, hpref, &n_heavy));
         k_cross_keys<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, view(g->fw), label, keys, flag);
         GIR_LAUNCH(g, "k_cross_keys");
+        if (n_heavy > 0) {
+            k_cross_keys_heavy<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(heavy, hpref, n_heavy, view(g->fw), label,
+                                                                               keys, flag);
+            GIR_LAUNCH(g, "k_cross_keys_heavy");
+        }
     }
     int64_t n_cross = 0;
     GIR_TRY(select_flagged_u64(g, keys, flag, tmp, cap, &n_cross));

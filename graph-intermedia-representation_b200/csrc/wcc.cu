@@ -45,14 +45,6 @@ __device__ __forceinline__ void uf_link(int32_t* parent, int32_t a, int32_t b, i
 
 __global__ void k_uf_init(int32_t* parent, int64_t V) { GRID_STRIDE(v, V) parent[v] = (int32_t)v; }
 
-__global__ void __launch_bounds__(kBlock) k_uf_link_rows(CSRView c, int64_t V, int32_t* parent, int32_t* err) {
-    __shared__ int64_t s_excl[kBlock / 32][33];
-    __shared__ int32_t s_u[kBlock / 32][32];
-    const int wib = threadIdx.x >> 5;
-    warp_sweep_rows(c.beg, c.deg, c.adj, 0, V, s_excl[wib], s_u[wib],
-                    [&](int32_t u, int32_t w, int64_t) { uf_link(parent, u, w, err); });
-}
-
 // Links the endpoints of every pair key (u << 32 | v) into the existing forest.
 __global__ void k_uf_link_keys(const uint64_t* keys, int64_t n, int32_t* parent, int32_t* err) {
     GRID_STRIDE(i, n) uf_link(parent, (int32_t)(keys[i] >> 32), (int32_t)(keys[i] & 0xffffffffULL), err);

@@ -172,9 +172,9 @@ struct Relax {
     unsigned long long* setmask;   // lanes settled in this bucket
     int32_t* setq;
     // Lanes whose distance is final: those settled in buckets whose light phase is over (their
-    // heavy pass ORs them in). A relaxation always carries at least the current bucket's start,
-    // so it can never lower a final lane: the pair is dropped on this 8-byte-per-vertex mask
-    // (38 MB on the 4.8M-vertex graph, L2-resident) without reading the lane's distance.
+    // heavy pass ORs them in). k_far_split drops such lanes from the far set without reading
+    // their distances. (k_relax does not test it: on R-MAT graphs the extra 8-byte load per edge
+    // cost more than the distance reads and atomics it saved.)
     unsigned long long* done;
     unsigned long long* cnt;
 };
@@ -273,6 +273,39 @@ __device__ __forceinline__ int64_t warp_search(const int64_t* pref, int64_t lo, 
     return lo;
 }
 
+// Relaxes the pairs this thread holds (pair j: on[j], target w[j], lane sl[j], the source's lane
+// distance du[j], edge weight wt[j]); the queue appends are staged per warp (warp-uniform call).
+template <class D>
+__device__ __forceinline__ void relax_held(D* dist, const Relax& a, const bool (&on)[kPairs], const int32_t (&w)[kPairs],
+                                           const int32_t (&sl)[kPairs], const uint64_t (&du)[kPairs],
+                                           const uint32_t (&wt)[kPairs], int32_t* s_near, int& n_near, int32_t* s_far,
+                                           int& n_far) {
+    uint64_t cur[kPairs];
+#pragma unroll
+    for (int j = 0; j < kPairs; ++j)
+        cur[j] = on[j] ? *(volatile D*)&dist[(int64_t)w[j] * a.nl + sl[j]] : (D)0;
+#pragma unroll
+    for (int j = 0; j < kPairs; ++j) {
+        bool to_near = false, to_far = false;
+        if (on[j]) {
+            const uint64_t nd = du[j] + (uint64_t)wt[j];
+            if (sizeof(D) == 2 && nd >= (uint64_t)DistT<D>::inf) {
+                // a 16-bit lane cannot hold it: the group is run again with 32-bit lanes
+                if (cur[j] == (uint64_t)DistT<D>::inf) a.cnt[S_OVF] = 1ull;
+            } else if (nd < cur[j]) {  // plain pre-check: most relaxations lose
+                const uint64_t old = DistT<D>::atomic_min(&dist[(int64_t)w[j] * a.nl + sl[j]], (D)nd);
+                if (nd < old) {
+                    const unsigned long long bit = 1ull << sl[j];
+                    if (nd < a.kend) to_near = atomicOr(&a.nextmask[w[j]], bit) == 0ull;
+                    else to_far = atomicOr(&a.farmask[w[j]], bit) == 0ull;
+                }
+            }
+        }
+        stage_append(to_near, w[j], s_near, n_near, a.nextq, &a.cnt[S_NEAR]);
+        stage_append(to_far, w[j], s_far, n_far, a.farq, &a.cnt[S_FAR]);
+    }
+}
+
 // Load-balanced relaxation over all (edge, lane) pairs of the item list, numbered by the
 // exclusive scan of the items' work. Every warp takes one contiguous run of pairs and finds the
 // item holding its first pair with one warp search. It then walks windows of 32 consecutive
@@ -280,6 +313,13 @@ __device__ __forceinline__ int64_t warp_search(const int64_t* pref, int64_t lo, 
 // window through shuffles, so no shared memory and no block barrier is involved and warps
 // proceed independently. Pairs are enumerated edge-major within an item: with many lanes
 // active, consecutive threads update consecutive lanes of one distance row.
+//
+// Where the warp's next steps (32 * kPairs pairs each) all lie inside one item (a hub's row,
+// settled in many lanes at once: a few such items hold most of the pairs of the early heavy
+// passes), the warp leaves the per-pair search: each thread divides its first pair's rank once,
+// then steps its (edge, lane rank) position by the constant 32 * kPairs, and takes the lane from
+// a table of the item's set lanes held one per thread (two shuffles instead of a search, a divide
+// and a find-n-th-bit per pair). The pairs relaxed are the same either way.
 template <class D>
 __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long long* n_items, Items it, Relax a) {
     D* const dist = static_cast<D*>(a.dist);
@@ -287,6 +327,8 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
     if (n == 0) return;
     const int64_t total = it.pref[n];
     __shared__ int32_t s_near[kRelaxThreads / 32][kStage], s_far[kRelaxThreads / 32][kStage];
+    int32_t* const my_near = s_near[threadIdx.x >> 5];
+    int32_t* const my_far = s_far[threadIdx.x >> 5];
     int n_near = 0, n_far = 0;
     const int ln = lane_id();
     const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -295,6 +337,7 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
     const int64_t c0 = gw * per;
     const int64_t c1 = c0 + per < total ? c0 + per : total;
     if (c0 >= c1) return;
+    constexpr int kStep = 32 * kPairs;
     int64_t e0 = warp_search(it.pref, 0, n - 1, c0);
     int64_t p = c0;
     while (p < c1) {
@@ -311,7 +354,60 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
         }
         const int64_t wnext = e0 + 32 < n ? it.pref[e0 + 32] : total;
         const int64_t wend = wnext < c1 ? wnext : c1;
-        for (; p < wend; p += 32 * kPairs) {
+        while (p < wend) {
+            {
+                // the item holding pair p (the same for every thread) and where its run ends
+                int x = 0;
+#pragma unroll
+                for (int b = 16; b; b >>= 1) {
+                    const int64_t v = __shfl_sync(0xffffffffu, pj, x + b);
+                    if (v <= p) x += b;
+                }
+                const int64_t pn = __shfl_sync(0xffffffffu, pj, (x + 1) & 31);
+                const int64_t xend = x < 31 ? (pn < wend ? pn : wend) : wend;
+                if (xend - p >= 2 * kStep) {
+                    const int64_t px = __shfl_sync(0xffffffffu, pj, x);
+                    const int64_t ebx = __shfl_sync(0xffffffffu, ebj, x);
+                    const unsigned long long mx = __shfl_sync(0xffffffffu, mj, x);
+                    const int64_t urow = (int64_t)__shfl_sync(0xffffffffu, uj, x) * a.nl;
+                    const int pc = __popcll(mx);
+                    const int32_t sel_lo = ln < pc ? nth_bit(mx, ln) : 0;
+                    const int32_t sel_hi = ln + 32 < pc ? nth_bit(mx, ln + 32) : 0;
+                    const int da = kStep / pc, db = kStep % pc;
+                    int64_t e[kPairs];
+                    int r[kPairs];
+#pragma unroll
+                    for (int j = 0; j < kPairs; ++j) {
+                        const int64_t q2 = p + j * 32 + ln - px;
+                        e[j] = q2 / pc;
+                        r[j] = (int)(q2 - e[j] * pc);
+                    }
+                    for (; p + kStep <= xend; p += kStep) {
+                        bool on[kPairs];
+                        int32_t w[kPairs], sl[kPairs];
+                        uint64_t du[kPairs];
+                        uint32_t wt[kPairs];
+#pragma unroll
+                        for (int j = 0; j < kPairs; ++j) {
+                            const int32_t lo = __shfl_sync(0xffffffffu, sel_lo, r[j] & 31);
+                            const int32_t hi = __shfl_sync(0xffffffffu, sel_hi, r[j] & 31);
+                            sl[j] = r[j] < 32 ? lo : hi;
+                            on[j] = true;
+                            w[j] = __ldcs(&a.wadj[ebx + e[j]]);
+                            wt[j] = __ldcs(&a.ww[ebx + e[j]]);
+                            du[j] = dist[urow + sl[j]];
+                            e[j] += da;
+                            r[j] += db;
+                            if (r[j] >= pc) {
+                                r[j] -= pc;
+                                e[j] += 1;
+                            }
+                        }
+                        relax_held<D>(dist, a, on, w, sl, du, wt, my_near, n_near, my_far, n_far);
+                    }
+                    continue;  // (what is left of the item, under one step, goes the general way)
+                }
+            }
             int32_t w[kPairs], sl[kPairs];
             int64_t k[kPairs];
             uint64_t du[kPairs];
@@ -343,39 +439,14 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
             for (int j = 0; j < kPairs; ++j) {
                 if (on[j]) { w[j] = __ldcs(&a.wadj[k[j]]); wt[j] = __ldcs(&a.ww[k[j]]); } else { w[j] = 0; wt[j] = 0; }
             }
-#pragma unroll
-            for (int j = 0; j < kPairs; ++j)
-                if (on[j] && ((a.done[w[j]] >> sl[j]) & 1ull)) on[j] = false;
-            uint64_t cur[kPairs];
-#pragma unroll
-            for (int j = 0; j < kPairs; ++j)
-                cur[j] = on[j] ? *(volatile D*)&dist[(int64_t)w[j] * a.nl + sl[j]] : (D)0;
-#pragma unroll
-            for (int j = 0; j < kPairs; ++j) {
-                bool to_near = false, to_far = false;
-                if (on[j]) {
-                    const uint64_t nd = du[j] + (uint64_t)wt[j];
-                    if (sizeof(D) == 2 && nd >= (uint64_t)DistT<D>::inf) {
-                        // a 16-bit lane cannot hold it: the group is run again with 32-bit lanes
-                        if (cur[j] == (uint64_t)DistT<D>::inf) a.cnt[S_OVF] = 1ull;
-                    } else if (nd < cur[j]) {  // plain pre-check: most relaxations lose
-                        const uint64_t old = DistT<D>::atomic_min(&dist[(int64_t)w[j] * a.nl + sl[j]], (D)nd);
-                        if (nd < old) {
-                            const unsigned long long bit = 1ull << sl[j];
-                            if (nd < a.kend) to_near = atomicOr(&a.nextmask[w[j]], bit) == 0ull;
-                            else to_far = atomicOr(&a.farmask[w[j]], bit) == 0ull;
-                        }
-                    }
-                }
-                stage_append(to_near, w[j], s_near[threadIdx.x >> 5], n_near, a.nextq, &a.cnt[S_NEAR]);
-                stage_append(to_far, w[j], s_far[threadIdx.x >> 5], n_far, a.farq, &a.cnt[S_FAR]);
-            }
+            relax_held<D>(dist, a, on, w, sl, du, wt, my_near, n_near, my_far, n_far);
+            p += kStep;
         }
         p = wend;  // (the pairs of this window end exactly where item e0+32 begins)
         e0 += 32;
     }
-    stage_flush(s_near[threadIdx.x >> 5], n_near, a.nextq, &a.cnt[S_NEAR]);
-    stage_flush(s_far[threadIdx.x >> 5], n_far, a.farq, &a.cnt[S_FAR]);
+    stage_flush(my_near, n_near, a.nextq, &a.cnt[S_NEAR]);
+    stage_flush(my_far, n_far, a.farq, &a.cnt[S_FAR]);
 }
 
 // Splits the far entries at the bucket [lo, hi): lanes inside it become near work, later lanes

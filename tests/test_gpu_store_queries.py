@@ -274,7 +274,17 @@ def test_betweenness_matches_reference(pkg, orc, s16):
     another order than the reference's, so the bar is a relative 1e-9."""
     small = pkg.graphs.rmat(12, seed=14, weights=None)
     g, _, _ = s16
-    for gr, n in ((small, 70), (g, 100)):
+    # Rows longer than 4,096 entries are summed in 1,024-entry chunks: vertex 0 points to 6,001
+    # vertices, 6,001 vertices point to vertex 1, over a sparse random graph of 3 out-edges each.
+    rng = np.random.default_rng(21)
+    V = 12_000
+    su = np.concatenate([np.repeat(np.arange(V, dtype=np.int64), 3), np.zeros(6001, np.int64),
+                         np.arange(2, 6003)])
+    sv = np.concatenate([rng.integers(0, V, 3 * V), np.arange(V - 6001, V), np.ones(6001, np.int64)])
+    key = np.unique(su * V + sv)
+    hubs = pkg.graphs.from_edges(V, key // V, key % V, name="hubs")
+    assert np.diff(hubs.fw_beg).max() > 4096 and np.diff(hubs.bw_beg).max() > 4096
+    for gr, n in ((small, 70), (g, 100), (hubs, 80)):
         d = pkg.DeviceGraph.from_graph(gr, weights=False)
         src = np.concatenate([pkg.graphs.sources_with_edges(gr, n, 3), [0, 0, -5, gr.V + 2]]).astype(np.int32)
         got = d.bc(src)

@@ -223,19 +223,22 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
         int64_t eb = 0, work = 0;
         bool settles = false;
         if (i < n) {
+            // (every load of the vertex's words is issued before any store: the stores may alias
+            // them for all the compiler knows, and would otherwise serialize three DRAM latencies)
             u = q[i];
+            const int4 r = rows[u];
             if (heavy) {
                 m = a.setmask[u];
+                const unsigned long long dn = a.done[u];
                 a.setmask[u] = 0ull;
-                a.done[u] |= m;  // (u appears once in a heavy pass)
+                a.done[u] = dn | m;  // (u appears once in a heavy pass)
             } else {
                 m = a.curmask[u];
-                a.curmask[u] = 0ull;
                 const unsigned long long old = a.setmask[u];
+                a.curmask[u] = 0ull;
                 a.setmask[u] = old | m;
                 settles = m && old == 0ull;
             }
-            const int4 r = rows[u];
             const int64_t b = (int64_t)(((uint64_t)(uint32_t)r.y << 32) | (uint32_t)r.x);
             const int32_t nlu = r.w;
             eb = heavy ? b + nlu : b;
@@ -428,9 +431,11 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
                 const int32_t ux = __shfl_sync(0xffffffffu, uj, x);
                 if (on[j]) {
                     const int pc = __popcll(mx);
-                    const int32_t q2 = (int32_t)(q - px);
-                    k[j] = ebx + q2 / pc;
-                    sl[j] = nth_bit(mx, q2 % pc);
+                    const int64_t q2 = q - px;
+                    // (an item of 2^31 pairs or more, a row of over 2^25 entries, takes the wide divide)
+                    const int64_t ed = q2 <= INT32_MAX ? (int64_t)((uint32_t)q2 / (uint32_t)pc) : q2 / pc;
+                    k[j] = ebx + ed;
+                    sl[j] = nth_bit(mx, (int)(q2 - ed * pc));
                     du[j] = dist[(int64_t)ux * a.nl + sl[j]];
                 }
             }
@@ -459,29 +464,51 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
     const int64_t n = (int64_t)*nfar;
     __shared__ int32_t s_near[kBlock / 32][kStage], s_far[kBlock / 32][kStage];
     int n_near = 0, n_far = 0;
+    const int ln = lane_id();
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
-        bool to_near = false, to_far = false;
         int32_t w = 0;
-        unsigned long long mn = kInf;
+        unsigned long long m = 0;
         if (i < n) {
             w = farq[i];
             // (lanes already final were reached by a shorter path since: dropped unread)
-            unsigned long long m = farmask[w] & ~done[w], nm = 0, keep = 0;
-            while (m) {
-                const int s = __ffsll((long long)m) - 1;
-                m &= m - 1;
-                const uint64_t d = dist[(int64_t)w * nl + s];
-                if (d >= lo && d < hi) {
-                    nm |= 1ull << s;
-                } else if (d >= hi) {
-                    keep |= 1ull << s;
-                    mn = d < mn ? d : mn;
-                }
+            m = farmask[w] & ~done[w];
+        }
+        // The warp takes its 32 entries in turn and reads each entry's distance row once, lanes
+        // ln and ln + 32 per thread (coalesced); ballots give the entry's near and kept lanes.
+        unsigned long long mn = kInf, my_near = 0, my_keep = 0;
+#pragma unroll 4
+        for (int j = 0; j < 32; ++j) {
+            const unsigned long long mj = __shfl_sync(0xffffffffu, m, j);
+            if (mj == 0ull) continue;  // (warp-uniform)
+            const int64_t row = (int64_t)__shfl_sync(0xffffffffu, w, j) * nl;
+            bool n0 = false, n1 = false, k0 = false, k1 = false;
+            if ((mj >> ln) & 1ull) {
+                const uint64_t d = dist[row + ln];
+                n0 = d >= lo && d < hi;
+                k0 = d >= hi;
+                if (k0) mn = d < mn ? d : mn;
             }
-            farmask[w] = keep;
-            to_far = keep != 0;
-            if (nm) to_near = atomicOr(&nearmask[w], nm) == 0ull;
+            if ((mj >> 32 >> ln) & 1ull) {
+                const uint64_t d = dist[row + 32 + ln];
+                n1 = d >= lo && d < hi;
+                k1 = d >= hi;
+                if (k1) mn = d < mn ? d : mn;
+            }
+            const unsigned long long nm = (unsigned long long)__ballot_sync(0xffffffffu, n0) |
+                                          ((unsigned long long)__ballot_sync(0xffffffffu, n1) << 32);
+            const unsigned long long kp = (unsigned long long)__ballot_sync(0xffffffffu, k0) |
+                                          ((unsigned long long)__ballot_sync(0xffffffffu, k1) << 32);
+            if (ln == j) {
+                my_near = nm;
+                my_keep = kp;
+            }
+        }
+        bool to_near = false, to_far = false;
+        if (i < n) {
+            farmask[w] = my_keep;
+            to_far = my_keep != 0ull;
+            if (my_near) to_near = atomicOr(&nearmask[w], my_near) == 0ull;
         }
         stage_append(to_near, w, s_near[threadIdx.x >> 5], n_near, nearq, &cnt[S_NEAR]);
         stage_append(to_far, w, s_far[threadIdx.x >> 5], n_far, farq2, &cnt[S_FAR2]);
@@ -489,7 +516,7 @@ __global__ void k_far_split(const int32_t* farq, const unsigned long long* nfar,
             const unsigned long long t = __shfl_xor_sync(0xffffffffu, mn, o);
             mn = t < mn ? t : mn;
         }
-        if (lane_id() == 0 && mn != kInf) atomicMin(&cnt[S_MIN], mn);
+        if (ln == 0 && mn != kInf) atomicMin(&cnt[S_MIN], mn);
     }
     stage_flush(s_near[threadIdx.x >> 5], n_near, nearq, &cnt[S_NEAR]);
     stage_flush(s_far[threadIdx.x >> 5], n_far, farq2, &cnt[S_FAR2]);

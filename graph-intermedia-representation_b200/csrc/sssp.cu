@@ -258,7 +258,12 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
 }
 
 constexpr int kRelaxThreads = 256;
-constexpr int kPairs = 2;  // pairs in flight per thread (with 6 CTAs per SM: measured best)
+// Pairs per thread per step, and CTAs per SM: latency-bound, so occupancy wins. Measured on the
+// 4.8M-vertex R-MAT (64 lanes): 1 pair at 8 CTAs (32 registers) 71 ms per call, 7 CTAs the same,
+// 6 CTAs 75 ms, 4 CTAs 83 ms; 2 pairs at 6 CTAs 74 ms, at 5 CTAs 76 ms.
+constexpr int kPairs = 1;
+constexpr int kRelaxMinBlocks = 8;
+constexpr int kDeal = 16;  // chunks of pairs per warp and launch (a chunk is at least 32 pairs)
 
 // Largest e in [lo, hi] with pref[e] <= key, for a non-decreasing pref with pref[lo] <= key
 // (the probes at or below the key are a prefix of each round's 32). One warp, 32 probes a round:
@@ -324,7 +329,7 @@ __device__ __forceinline__ void relax_held(D* dist, const Relax& a, const bool (
 // a table of the item's set lanes held one per thread (two shuffles instead of a search, a divide
 // and a find-n-th-bit per pair). The pairs relaxed are the same either way.
 template <class D>
-__global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long long* n_items, Items it, Relax a) {
+__global__ void __launch_bounds__(kRelaxThreads, kRelaxMinBlocks) k_relax(const unsigned long long* n_items, Items it, Relax a) {
     D* const dist = static_cast<D*>(a.dist);
     const int64_t n = (int64_t)*n_items;
     if (n == 0) return;
@@ -336,119 +341,130 @@ __global__ void __launch_bounds__(kRelaxThreads, 6) k_relax(const unsigned long 
     const int ln = lane_id();
     const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t per = (((total + nw - 1) / nw) + 31) & ~(int64_t)31;
-    const int64_t c0 = gw * per;
-    const int64_t c1 = c0 + per < total ? c0 + per : total;
-    if (c0 >= c1) return;
     constexpr int kStep = 32 * kPairs;
-    int64_t e0 = warp_search(it.pref, 0, n - 1, c0);
-    int64_t p = c0;
-    while (p < c1) {
-        // window: items e0 .. e0+31, lane j holding item e0+j
-        const int64_t ej = e0 + ln;
-        int64_t pj = INT64_MAX, ebj = 0;
-        unsigned long long mj = 0;
-        int32_t uj = 0;
-        if (ej < n) {
-            pj = it.pref[ej];
-            ebj = it.eb[ej];
-            mj = it.m[ej];
-            uj = it.u[ej];
-        }
-        const int64_t wnext = e0 + 32 < n ? it.pref[e0 + 32] : total;
-        const int64_t wend = wnext < c1 ? wnext : c1;
-        while (p < wend) {
-            {
-                // the item holding pair p (the same for every thread) and where its run ends
-                int x = 0;
-#pragma unroll
-                for (int b = 16; b; b >>= 1) {
-                    const int64_t v = __shfl_sync(0xffffffffu, pj, x + b);
-                    if (v <= p) x += b;
+    // The pairs are dealt in chunks, round-robin over the warps (about kDeal chunks per warp), so
+    // every warp gets a mix of cheap pairs (long items, the fast path below) and costly ones
+    // (short items): one contiguous run per warp left the warps inside short items running
+    // 1.75x longer than the average SM in the first heavy passes.
+    const int64_t chunk = (((total + nw * kDeal - 1) / (nw * kDeal)) + 31) & ~(int64_t)31;
+    int64_t e_from = 0;  // (a warp's chunks ascend: each search starts at the previous chunk's item)
+    for (int64_t c0 = gw * chunk; c0 < total; c0 += nw * chunk) {
+        const int64_t c1 = c0 + chunk < total ? c0 + chunk : total;
+        int64_t e0 = warp_search(it.pref, e_from, n - 1, c0);
+        e_from = e0;
+        int64_t p = c0;
+        while (p < c1) {
+            // window: items e0 .. e0+31, lane j holding item e0+j
+            const int64_t ej = e0 + ln;
+            int64_t pj = INT64_MAX, ebj = 0;
+            unsigned long long mj = 0;
+            int32_t uj = 0;
+            if (ej < n) {
+                pj = it.pref[ej];
+                ebj = it.eb[ej];
+                mj = it.m[ej];
+                uj = it.u[ej];
+            }
+            const int64_t wnext = e0 + 32 < n ? it.pref[e0 + 32] : total;
+            const int64_t wend = wnext < c1 ? wnext : c1;
+            while (p < wend) {
+                {
+                    // the item holding pair p (the same for every thread) and where its run ends
+                    int x = 0;
+    #pragma unroll
+                    for (int b = 16; b; b >>= 1) {
+                        const int64_t v = __shfl_sync(0xffffffffu, pj, x + b);
+                        if (v <= p) x += b;
+                    }
+                    const int64_t pn = __shfl_sync(0xffffffffu, pj, (x + 1) & 31);
+                    const int64_t xend = x < 31 ? (pn < wend ? pn : wend) : wend;
+                    if (xend - p >= 2 * kStep) {
+                        const int64_t px = __shfl_sync(0xffffffffu, pj, x);
+                        const int64_t ebx = __shfl_sync(0xffffffffu, ebj, x);
+                        const unsigned long long mx = __shfl_sync(0xffffffffu, mj, x);
+                        const int64_t urow = (int64_t)__shfl_sync(0xffffffffu, uj, x) * a.nl;
+                        const int pc = __popcll(mx);
+                        const int32_t sel_lo = ln < pc ? nth_bit(mx, ln) : 0;
+                        const int32_t sel_hi = ln + 32 < pc ? nth_bit(mx, ln + 32) : 0;
+                        const int da = kStep / pc, db = kStep % pc;
+                        int64_t e[kPairs];
+                        int r[kPairs];
+    #pragma unroll
+                        for (int j = 0; j < kPairs; ++j) {
+                            const int64_t q2 = p + j * 32 + ln - px;
+                            e[j] = q2 / pc;
+                            r[j] = (int)(q2 - e[j] * pc);
+                        }
+                        for (; p + kStep <= xend; p += kStep) {
+                            bool on[kPairs];
+                            int32_t w[kPairs], sl[kPairs];
+                            uint64_t du[kPairs];
+                            uint32_t wt[kPairs];
+    #pragma unroll
+                            for (int j = 0; j < kPairs; ++j) {
+                                const int32_t lo = __shfl_sync(0xffffffffu, sel_lo, r[j] & 31);
+                                const int32_t hi = __shfl_sync(0xffffffffu, sel_hi, r[j] & 31);
+                                sl[j] = r[j] < 32 ? lo : hi;
+                                on[j] = true;
+                                w[j] = __ldcs(&a.wadj[ebx + e[j]]);
+                                wt[j] = __ldcs(&a.ww[ebx + e[j]]);
+                                du[j] = dist[urow + sl[j]];
+                                e[j] += da;
+                                r[j] += db;
+                                if (r[j] >= pc) {
+                                    r[j] -= pc;
+                                    e[j] += 1;
+                                }
+                            }
+                            relax_held<D>(dist, a, on, w, sl, du, wt, my_near, n_near, my_far, n_far);
+                        }
+                        continue;  // (what is left of the item, under one step, goes the general way)
+                    }
                 }
-                const int64_t pn = __shfl_sync(0xffffffffu, pj, (x + 1) & 31);
-                const int64_t xend = x < 31 ? (pn < wend ? pn : wend) : wend;
-                if (xend - p >= 2 * kStep) {
+                int32_t w[kPairs], sl[kPairs];
+                int64_t k[kPairs];
+                uint64_t du[kPairs];
+                bool on[kPairs];
+    #pragma unroll
+                for (int j = 0; j < kPairs; ++j) {
+                    const int64_t q = p + j * 32 + ln;
+                    on[j] = q < wend;
+                    int x = 0;  // largest x with pref(x) <= q
+    #pragma unroll
+                    for (int b = 16; b; b >>= 1) {
+                        const int64_t v = __shfl_sync(0xffffffffu, pj, x + b);
+                        if (v <= q) x += b;
+                    }
                     const int64_t px = __shfl_sync(0xffffffffu, pj, x);
                     const int64_t ebx = __shfl_sync(0xffffffffu, ebj, x);
                     const unsigned long long mx = __shfl_sync(0xffffffffu, mj, x);
-                    const int64_t urow = (int64_t)__shfl_sync(0xffffffffu, uj, x) * a.nl;
-                    const int pc = __popcll(mx);
-                    const int32_t sel_lo = ln < pc ? nth_bit(mx, ln) : 0;
-                    const int32_t sel_hi = ln + 32 < pc ? nth_bit(mx, ln + 32) : 0;
-                    const int da = kStep / pc, db = kStep % pc;
-                    int64_t e[kPairs];
-                    int r[kPairs];
-#pragma unroll
-                    for (int j = 0; j < kPairs; ++j) {
-                        const int64_t q2 = p + j * 32 + ln - px;
-                        e[j] = q2 / pc;
-                        r[j] = (int)(q2 - e[j] * pc);
+                    const int32_t ux = __shfl_sync(0xffffffffu, uj, x);
+                    if (on[j]) {
+                        const int pc = __popcll(mx);
+                        const int64_t q2 = q - px;
+                        // (an item of 2^31 pairs or more, a row of over 2^25 entries, takes the wide divide)
+                        const int64_t ed = q2 <= INT32_MAX ? (int64_t)((uint32_t)q2 / (uint32_t)pc) : q2 / pc;
+                        k[j] = ebx + ed;
+                        sl[j] = nth_bit(mx, (int)(q2 - ed * pc));
+                        du[j] = dist[(int64_t)ux * a.nl + sl[j]];
                     }
-                    for (; p + kStep <= xend; p += kStep) {
-                        bool on[kPairs];
-                        int32_t w[kPairs], sl[kPairs];
-                        uint64_t du[kPairs];
-                        uint32_t wt[kPairs];
-#pragma unroll
-                        for (int j = 0; j < kPairs; ++j) {
-                            const int32_t lo = __shfl_sync(0xffffffffu, sel_lo, r[j] & 31);
-                            const int32_t hi = __shfl_sync(0xffffffffu, sel_hi, r[j] & 31);
-                            sl[j] = r[j] < 32 ? lo : hi;
-                            on[j] = true;
-                            w[j] = __ldcs(&a.wadj[ebx + e[j]]);
-                            wt[j] = __ldcs(&a.ww[ebx + e[j]]);
-                            du[j] = dist[urow + sl[j]];
-                            e[j] += da;
-                            r[j] += db;
-                            if (r[j] >= pc) {
-                                r[j] -= pc;
-                                e[j] += 1;
-                            }
-                        }
-                        relax_held<D>(dist, a, on, w, sl, du, wt, my_near, n_near, my_far, n_far);
-                    }
-                    continue;  // (what is left of the item, under one step, goes the general way)
                 }
-            }
-            int32_t w[kPairs], sl[kPairs];
-            int64_t k[kPairs];
-            uint64_t du[kPairs];
-            bool on[kPairs];
-#pragma unroll
-            for (int j = 0; j < kPairs; ++j) {
-                const int64_t q = p + j * 32 + ln;
-                on[j] = q < wend;
-                int x = 0;  // largest x with pref(x) <= q
-#pragma unroll
-                for (int b = 16; b; b >>= 1) {
-                    const int64_t v = __shfl_sync(0xffffffffu, pj, x + b);
-                    if (v <= q) x += b;
+                uint32_t wt[kPairs];
+    #pragma unroll
+                for (int j = 0; j < kPairs; ++j) {
+                    if (on[j]) { w[j] = __ldcs(&a.wadj[k[j]]); wt[j] = __ldcs(&a.ww[k[j]]); } else { w[j] = 0; wt[j] = 0; }
                 }
-                const int64_t px = __shfl_sync(0xffffffffu, pj, x);
-                const int64_t ebx = __shfl_sync(0xffffffffu, ebj, x);
-                const unsigned long long mx = __shfl_sync(0xffffffffu, mj, x);
-                const int32_t ux = __shfl_sync(0xffffffffu, uj, x);
-                if (on[j]) {
-                    const int pc = __popcll(mx);
-                    const int64_t q2 = q - px;
-                    // (an item of 2^31 pairs or more, a row of over 2^25 entries, takes the wide divide)
-                    const int64_t ed = q2 <= INT32_MAX ? (int64_t)((uint32_t)q2 / (uint32_t)pc) : q2 / pc;
-                    k[j] = ebx + ed;
-                    sl[j] = nth_bit(mx, (int)(q2 - ed * pc));
-                    du[j] = dist[(int64_t)ux * a.nl + sl[j]];
-                }
+                relax_held<D>(dist, a, on, w, sl, du, wt, my_near, n_near, my_far, n_far);
+                p += kStep;
             }
-            uint32_t wt[kPairs];
-#pragma unroll
-            for (int j = 0; j < kPairs; ++j) {
-                if (on[j]) { w[j] = __ldcs(&a.wadj[k[j]]); wt[j] = __ldcs(&a.ww[k[j]]); } else { w[j] = 0; wt[j] = 0; }
-            }
-            relax_held<D>(dist, a, on, w, sl, du, wt, my_near, n_near, my_far, n_far);
-            p += kStep;
+            p = wend;  // (the pairs of this window end exactly where item e0+32 begins)
+            if (p >= c1) break;
+            // Items without work keep their slots (their prefix equals the next item's): where the
+            // whole next window is such items, jump past the run with one search instead of
+            // walking it 32 items at a time (a heavy pass on a lattice can hold millions of them).
+            const int64_t nx = e0 + 32;
+            e0 = nx + 32 < n && it.pref[nx + 32] <= p ? warp_search(it.pref, nx, n - 1, p) : nx;
         }
-        p = wend;  // (the pairs of this window end exactly where item e0+32 begins)
-        e0 += 32;
     }
     stage_flush(my_near, n_near, a.nextq, &a.cnt[S_NEAR]);
     stage_flush(my_far, n_far, a.farq, &a.cnt[S_FAR]);

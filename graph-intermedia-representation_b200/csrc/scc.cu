@@ -147,22 +147,26 @@ __global__ void k_pivot(int64_t V, const int32_t* label, const int32_t* indeg, c
     }
 }
 
-// Edge-balanced reach (the pivot's forward / backward search): the frontier's rows are cut into
-// equal chunks after a scan of their lengths, so hubs do not serialize a warp.
-//   forward:  w joins when unassigned and not yet marked `epoch` (it gets the mark);
-//   backward: w joins when marked `epoch` by the forward search and still unassigned (it gets
-//             the pivot's label: FW ∩ BW = SCC(pivot)).
-__global__ void k_frontier_deg(const int32_t* q, int64_t n, const int32_t* deg, int64_t* pref) {
-    GRID_STRIDE(i, n) pref[i] = deg[q[i]];
+// Edge-balanced reach from the pivot, both directions in one level-synchronous traversal: a
+// queue entry e >= 0 is vertex e searched forward (out-rows), e < 0 is vertex ~e searched
+// backward (in-rows). The frontier's rows are cut into equal chunks after a scan of their
+// lengths, so hubs do not serialize a warp. An unassigned w joins a direction once (mark bit 1
+// forward, 2 backward); afterwards the vertices with both bits are SCC(pivot). Paths inside the
+// pivot's SCC never pass through trimmed (already labelled) vertices, so restricting both searches
+// to unassigned vertices keeps FW ∩ BW exact.
+__global__ void k_frontier_deg(const int32_t* q, int64_t n, const int32_t* fdeg, const int32_t* bdeg, int64_t* pref) {
+    GRID_STRIDE(i, n) {
+        const int32_t e = q[i];
+        pref[i] = e >= 0 ? fdeg[e] : bdeg[~e];
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) pref[n] = 0;
 }
 
 constexpr int kReachChunk = 32 * 16;
 
-template <bool Backward>
-__global__ void __launch_bounds__(kBlock) k_reach_balanced(const int32_t* q, int64_t nq, const int64_t* pref, CSRView c,
-                                                           int32_t* label, int32_t* mark, int32_t epoch, int32_t pivot,
-                                                           int32_t* out, unsigned long long* cnt) {
+__global__ void __launch_bounds__(kBlock) k_reach_both(const int32_t* q, int64_t nq, const int64_t* pref, CSRView fw,
+                                                       CSRView bw, const int32_t* label, int32_t* mark, int32_t* out,
+                                                       unsigned long long* cnt) {
     __shared__ int32_t s_st[kBlock / 32][kStage];
     int n_st = 0;
     const int64_t total = pref[nq];
@@ -181,21 +185,26 @@ __global__ void __launch_bounds__(kBlock) k_reach_balanced(const int32_t* q, int
         for (int64_t base = c0; base < c1; base += 32) {
             const int64_t p = base + lane;
             bool push = false;
-            int32_t w = 0;
+            int32_t ent = 0;
             if (p < c1) {
                 while (pref[i + 1] <= p) ++i;
-                const int32_t u = q[i];
-                w = c.adj[c.beg[u] + (p - pref[i])];
-                if (!Backward) {
-                    if (label[w] == -1 && mark[w] != epoch) push = atomicExch(&mark[w], epoch) != epoch;
-                } else {
-                    if (mark[w] == epoch && label[w] == -1) push = atomicCAS(&label[w], -1, pivot) == -1;
-                }
+                const int32_t e = q[i];
+                const bool back = e < 0;
+                const int32_t u = back ? ~e : e;
+                const int32_t w = back ? bw.adj[bw.beg[u] + (p - pref[i])] : fw.adj[fw.beg[u] + (p - pref[i])];
+                const int32_t bit = back ? 2 : 1;
+                if (label[w] == -1 && (mark[w] & bit) == 0) push = (atomicOr(&mark[w], bit) & bit) == 0;
+                ent = back ? ~w : w;
             }
-            stage_append(push, w, s_st[threadIdx.x >> 5], n_st, out, &cnt[C_Q]);
+            stage_append(push, ent, s_st[threadIdx.x >> 5], n_st, out, &cnt[C_Q]);
         }
     }
     stage_flush(s_st[threadIdx.x >> 5], n_st, out, &cnt[C_Q]);
+}
+
+// SCC(pivot): the unassigned vertices reached both ways.
+__global__ void k_reach_label(int64_t V, const int32_t* mark, int32_t pivot, int32_t* label) {
+    GRID_STRIDE(v, V) if (mark[v] == 3 && label[v] == -1) label[v] = pivot;
 }
 
 // Colour propagation: colour(w) = max(colour(w), colour(u)) along forward edges between
@@ -360,8 +369,9 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
     unsigned long long* cnt = nullptr;
     GIR_TRY(ensure_n(g, g->scratch[0], V + 1, &indeg));
     GIR_TRY(ensure_n(g, g->scratch[1], V + 1, &outdeg));
-    GIR_TRY(ensure_n(g, g->scratch[2], V + 1, &qa));
-    GIR_TRY(ensure_n(g, g->scratch[3], V + 1, &qb));
+    // (the queues hold up to 2V entries in the two-way reach from the pivot)
+    GIR_TRY(ensure_n(g, g->scratch[2], 2 * V + 2, &qa));
+    GIR_TRY(ensure_n(g, g->scratch[3], 2 * V + 2, &qb));
     GIR_TRY(ensure_n(g, g->scratch[4], V + 1, &mark));
     GIR_TRY(ensure_n(g, g->scratch[5], V + 1, &color));
     GIR_TRY(ensure_n(g, g->scratch[6], 2 * C_N, &cnt));
@@ -455,38 +465,27 @@ int scc_labels(gir_dev* g, int32_t* label, int64_t* n_scc) {
     }
     if (rule != 3 && lp.hc[C_PIV] != 0) {
         const int32_t pivot = (int32_t)((lp.hc[C_PIV] - 1) & 0xffffffffULL);
-        const int32_t epoch = 1;
-        // forward reach (marks), seeded with the pivot
-        GIR_CUDA(g, cudaMemcpyAsync(mark + pivot, &epoch, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
-        GIR_CUDA(g, cudaMemcpyAsync(qa, &pivot, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
-        const unsigned long long one = 1;
-        GIR_CUDA(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, g->stream));
-        GIR_CUDA(g, cudaMemcpyAsync(&cnt[C_Q], &one, sizeof(one), cudaMemcpyHostToDevice, g->stream));
+        // both searches seeded with the pivot (marked both ways)
+        int32_t *fa = qa, *fb = qb;
         int64_t* pref = nullptr;
-        GIR_TRY(ensure_n(g, g->scratch[7], V + 2, &pref));
-        // level-synchronous, edge-balanced: frontier degrees, scan, chunked expansion
-        auto balanced = [&](const CSRView& c, bool backward) -> int {
-            int64_t n = 1;
-            while (n > 0) {
-                k_frontier_deg<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(qa, n, c.deg, pref);
-                GIR_LAUNCH(g, "k_frontier_deg");
-                GIR_TRY(exclusive_scan_i64(g, pref, pref, n + 1));
-                GIR_CUDA(g, cudaMemsetAsync(&cnt[C_Q], 0, sizeof(unsigned long long), g->stream));
-                if (backward)
-                    k_reach_balanced<true><<<grid, kBlock, 0, g->stream>>>(qa, n, pref, c, label, mark, epoch, pivot, qb, cnt);
-                else
-                    k_reach_balanced<false><<<grid, kBlock, 0, g->stream>>>(qa, n, pref, c, label, mark, epoch, pivot, qb, cnt);
-                GIR_LAUNCH(g, "k_reach_balanced");
-                std::swap(qa, qb);
-                GIR_TRY(lp.read(&n));
-            }
-            return GIR_OK;
-        };
-        GIR_TRY(balanced(fw, false));
-        // backward reach inside the forward set: SCC(pivot)
-        GIR_CUDA(g, cudaMemcpyAsync(label + pivot, &pivot, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
-        GIR_CUDA(g, cudaMemcpyAsync(qa, &pivot, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
-        GIR_TRY(balanced(bw, true));
+        GIR_TRY(ensure_n(g, g->scratch[7], 2 * V + 2, &pref));
+        const int32_t seed[2] = {pivot, ~pivot}, both = 3;
+        GIR_CUDA(g, cudaMemcpyAsync(mark + pivot, &both, sizeof(int32_t), cudaMemcpyHostToDevice, g->stream));
+        GIR_CUDA(g, cudaMemcpyAsync(fa, seed, sizeof(seed), cudaMemcpyHostToDevice, g->stream));
+        GIR_CUDA(g, cudaStreamSynchronize(g->stream));  // (seed is a host stack array)
+        int64_t n = 2;
+        while (n > 0) {
+            k_frontier_deg<<<grid_for(g, n, kBlock), kBlock, 0, g->stream>>>(fa, n, fw.deg, bw.deg, pref);
+            GIR_LAUNCH(g, "k_frontier_deg");
+            GIR_TRY(exclusive_scan_i64(g, pref, pref, n + 1));
+            GIR_CUDA(g, cudaMemsetAsync(&cnt[C_Q], 0, sizeof(unsigned long long), g->stream));
+            k_reach_both<<<grid, kBlock, 0, g->stream>>>(fa, n, pref, fw, bw, label, mark, fb, cnt);
+            GIR_LAUNCH(g, "k_reach_both");
+            std::swap(fa, fb);
+            GIR_TRY(lp.read(&n));
+        }
+        k_reach_label<<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(V, mark, pivot, label);
+        GIR_LAUNCH(g, "k_reach_label");
     }
 
     trace_mark(g, "scc: fw-bw");

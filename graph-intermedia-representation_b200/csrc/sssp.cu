@@ -263,7 +263,8 @@ constexpr int kRelaxThreads = 256;
 // 6 CTAs 75 ms, 4 CTAs 83 ms; 2 pairs at 6 CTAs 74 ms, at 5 CTAs 76 ms.
 constexpr int kPairs = 1;
 constexpr int kRelaxMinBlocks = 8;
-constexpr int kDeal = 16;  // chunks of pairs per warp and launch (a chunk is at least 32 pairs)
+constexpr int kDeal = 8;  // chunks of pairs per warp and launch, at least 32 pairs each (measured on
+                          // the 4.8M-vertex R-MAT: 4 or 8 68.4 ms per call, 16 69.5, 32 72.0)
 
 // Largest e in [lo, hi] with pref[e] <= key, for a non-decreasing pref with pref[lo] <= key
 // (the probes at or below the key are a prefix of each round's 32). One warp, 32 probes a round:

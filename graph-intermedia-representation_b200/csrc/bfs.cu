@@ -108,30 +108,7 @@ __device__ __forceinline__ unsigned long long ldcg_u64(const unsigned long long*
 
 // All CTAs of the cooperative launch meet here. Returns false once any CTA has flagged an error.
 __device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned long long* err) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* gen = bar + 32;
-        const unsigned int g0 = *gen;
-        __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 32, 1u);
-        } else {
-            unsigned int spins = 0;
-            while (*gen == g0) {
-                if (++spins > kBarrierSpins) {
-                    atomicExch(err, 1ull);
-                    break;
-                }
-                if ((spins & 63) == 0 && ldcg_u64(err) != 0ull) break;
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return ldcg_u64(err) == 0ull;
+    return grid_barrier(bar, err, kBarrierSpins);
 }
 
 // End of a phase: the CTA's warps empty their staging buffers with one queue reservation for the

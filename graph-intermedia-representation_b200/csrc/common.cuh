@@ -451,6 +451,37 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t* q
     if (pred) q[base + __popc(m & ((1u << lane_id()) - 1))] = value;
 }
 
+// Grid-wide barrier of a cooperative launch: every CTA meets here. `bar` holds the arrival count
+// at bar[0] and the generation at bar[32] (own 128-byte lines), zeroed by the host before the
+// launch. The wait is bounded: after `spins` polls a CTA sets *err and leaves; every CTA also
+// leaves once it sees *err set. Returns false once any CTA has flagged an error.
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned long long* err, unsigned spins_max) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = bar + 32;
+        const unsigned int g0 = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 32, 1u);
+        } else {
+            unsigned int spins = 0;
+            while (*gen == g0) {
+                if (++spins > spins_max) {
+                    atomicExch(err, 1ull);
+                    break;
+                }
+                if ((spins & 63) == 0 && __ldcg(err) != 0ull) break;
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return __ldcg(err) == 0ull;
+}
+
 // Staged queue appends: a warp collects its entries in a shared-memory buffer of kStage slots
 // and reserves queue space with one atomicAdd per buffer-full, instead of one per ballot, so
 // thousands of warps appending to one queue do not serialize on its counter. Every lane of the

@@ -6,7 +6,7 @@
 // distance, then by parent id), all ones = unreachable; and the edge keys (u << 32 | v) that
 // batches changed since the last update.
 //
-// Update, every step a grid-wide kernel over HBM-resident arrays:
+// Update, one cooperative launch over HBM-resident arrays whose phases are these steps:
 //  1. presence of every logged edge now (binary search of u's sorted forward row);
 //  2. invalidation: a deleted tree edge u -> v cuts v; the cut spreads down the dependence tree
 //     (out-neighbours whose parent is a cut vertex) level by level. All cut vertices land in one
@@ -15,7 +15,7 @@
 //     the candidate words);
 //  4. seeds: the re-seeded cut vertices and the heads of inserted edges that improve;
 //  5. propagation: frontier Bellman-Ford. A vertex is queued at most once per round (a flag
-//     set by compare-and-swap); the flags of a round's frontier are cleared in their own launch
+//     set by compare-and-swap); the flags of a round's frontier are cleared in their own phase
 //     before the round reads any distance, so an improvement that lands after a vertex has
 //     read its own distance finds the flag clear and queues it again.
 // Distances only fall during propagation and every word is the length of a real path, so the
@@ -83,133 +83,6 @@ __global__ void k_inc_tree(int64_t V, CSRView bw, const uint64_t* d, int32_t src
     }
 }
 
-// present[i] = the edge of key i is in the graph now.
-__global__ void k_inc_present(const uint64_t* keys, int64_t n, CSRView fw, uint8_t* present) {
-    GRID_STRIDE(i, n) {
-        const int32_t u = (int32_t)(keys[i] >> 32), v = (int32_t)(uint32_t)keys[i];
-        const int64_t b = fw.beg[u], e = b + fw.deg[u];
-        const int64_t k = lower_bound_dev(fw.adj, b, e, v);
-        present[i] = k < e && fw.adj[k] == v;
-    }
-}
-
-// Step 2 seeds (gir_query.cpp:934-940): a logged edge that is absent now and was v's tree edge.
-__global__ void k_inc_cut(const uint64_t* keys, const uint8_t* present, int64_t n, int32_t src, const uint64_t* st,
-                          uint32_t* flag, int32_t* cut, unsigned long long* cnt) {
-    __shared__ int32_t s_q[kBlock / 32][kStage];
-    int n_q = 0;
-    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = base + threadIdx.x;  // (block-uniform trip count: every lane joins the appends)
-        bool push = false;
-        int32_t v = 0;
-        if (i < n && !present[i]) {
-            const int32_t u = (int32_t)(keys[i] >> 32);
-            v = (int32_t)(uint32_t)keys[i];
-            const uint64_t k = st[v];
-            push = v != src && k != kNone && parent_of(k) == u && atomicCAS(&flag[v], FLAG_CLEAR, FLAG_CUT) == FLAG_CLEAR;
-        }
-        stage_append(push, v, s_q[threadIdx.x >> 5], n_q, cut, cnt);
-    }
-    stage_flush(s_q[threadIdx.x >> 5], n_q, cut, cnt);
-}
-
-// One level of the cut (gir_query.cpp:941-953): out-neighbours whose parent is a cut vertex
-// of the level, appended behind it in the same list.
-__global__ void k_inc_cut_level(const int32_t* level_q, int64_t n, CSRView fw, int32_t src, const uint64_t* st,
-                                uint32_t* flag, int32_t* cut, unsigned long long* cnt) {
-    warp_expand(level_q, n, fw, cut, cnt, [&](int32_t x, int32_t y) {
-        if (y == src) return false;
-        const uint64_t k = st[y];
-        return k != kNone && parent_of(k) == x && atomicCAS(&flag[y], FLAG_CLEAR, FLAG_CUT) == FLAG_CLEAR;
-    });
-}
-
-__global__ void k_inc_unset(const int32_t* cut, int64_t n, uint64_t* st) {
-    GRID_STRIDE(i, n) st[cut[i]] = kNone;
-}
-
-// Step 3 (gir_query.cpp:955-968): a cut vertex restarts from its best valid in-neighbour. One
-// warp per cut vertex; the cut vertices' own words (kNone or being rewritten) are skipped by flag.
-__global__ void k_inc_reseed(const int32_t* cut, int64_t n, CSRView bw, const uint32_t* flag, int weighted,
-                             uint64_t* st) {
-    const int ln = lane_id();
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t i = warp; i < n; i += nwarps) {
-        const int32_t x = cut[i];
-        const int64_t b = bw.beg[x], e = b + bw.deg[x];
-        uint64_t best = kNone;
-        for (int64_t k = b + ln; k < e; k += 32) {
-            const int32_t p = bw.adj[k];
-            if (flag[p] == FLAG_CUT) continue;
-            const uint64_t kp = st[p];
-            if (kp == kNone) continue;
-            const uint64_t c = pack((kp >> 32) + weight_of(weighted, p, x), p);
-            best = c < best ? c : best;
-        }
-        best = warp_min_u64(best);
-        if (ln == 0) st[x] = best;
-    }
-}
-
-// Step 4a (gir_query.cpp:969-972): the cut vertices' flags are cleared; the re-seeded ones are queued.
-__global__ void k_inc_seed_cut(const int32_t* cut, int64_t n, const uint64_t* st, uint32_t* flag, int32_t* q,
-                               unsigned long long* cnt) {
-    __shared__ int32_t s_q[kBlock / 32][kStage];
-    int n_q = 0;
-    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = base + threadIdx.x;
-        bool push = false;
-        int32_t x = 0;
-        if (i < n) {
-            x = cut[i];
-            push = st[x] != kNone;
-            flag[x] = push ? FLAG_QUEUED : FLAG_CLEAR;
-        }
-        stage_append(push, x, s_q[threadIdx.x >> 5], n_q, q, cnt);
-    }
-    stage_flush(s_q[threadIdx.x >> 5], n_q, q, cnt);
-}
-
-// Step 4b (gir_query.cpp:973-981): logged edges present now relax once.
-__global__ void k_inc_seed_edges(const uint64_t* keys, const uint8_t* present, int64_t n, int weighted, uint64_t* st,
-                                 uint32_t* flag, int32_t* q, unsigned long long* cnt) {
-    __shared__ int32_t s_q[kBlock / 32][kStage];
-    int n_q = 0;
-    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = base + threadIdx.x;
-        bool push = false;
-        int32_t v = 0;
-        if (i < n && present[i]) {
-            const int32_t u = (int32_t)(keys[i] >> 32);
-            v = (int32_t)(uint32_t)keys[i];
-            const uint64_t k = __ldcg(&st[u]);
-            if (k != kNone) {
-                const uint64_t c = pack((k >> 32) + weight_of(weighted, u, v), u);
-                push = c < atomicMin((unsigned long long*)&st[v], (unsigned long long)c) &&
-                       atomicCAS(&flag[v], FLAG_CLEAR, FLAG_QUEUED) == FLAG_CLEAR;
-            }
-        }
-        stage_append(push, v, s_q[threadIdx.x >> 5], n_q, q, cnt);
-    }
-    stage_flush(s_q[threadIdx.x >> 5], n_q, q, cnt);
-}
-
-__global__ void k_inc_unflag(const int32_t* q, int64_t n, uint32_t* flag) {
-    GRID_STRIDE(i, n) flag[q[i]] = FLAG_CLEAR;
-}
-
-// Step 5, one round (gir_query.cpp:983-995): every frontier vertex relaxes its out-edges with its
-// current word (read through L2: other CTAs lower it during the round).
-__global__ void k_inc_round(const int32_t* q, int64_t n, CSRView fw, int weighted, uint64_t* st, uint32_t* flag,
-                            int32_t* nq, unsigned long long* ncnt) {
-    warp_expand(q, n, fw, nq, ncnt, [&](int32_t x, int32_t y) {
-        const uint64_t c = pack((__ldcg(&st[x]) >> 32) + weight_of(weighted, x, y), x);
-        return c < __ldcg(&st[y]) && c < atomicMin((unsigned long long*)&st[y], (unsigned long long)c) &&
-               atomicCAS(&flag[y], FLAG_CLEAR, FLAG_QUEUED) == FLAG_CLEAR;
-    });
-}
-
 __global__ void k_inc_dist(const uint64_t* st, int64_t V, uint64_t* out) {
     GRID_STRIDE(v, V) {
         const uint64_t k = st[v];
@@ -217,13 +90,188 @@ __global__ void k_inc_dist(const uint64_t* st, int64_t V, uint64_t* out) {
     }
 }
 
-// Reads cnt[0] (after the stream's queued work).
-int read_count(gir_dev* g, const unsigned long long* cnt, unsigned long long* host, int64_t* out) {
-    GIR_CUDA(g, cudaMemcpyAsync(host, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g->stream));
-    GIR_CUDA(g, cudaStreamSynchronize(g->stream));
-    *out = (int64_t)host[0];
-    return GIR_OK;
+// The whole update in one cooperative launch: the phases below are those of the steps in the
+// file comment, separated by bounded grid barriers instead of launches and host reads (a small
+// update's cost was its round trips: a cut level or a propagation round each waited for the
+// host). Counts live in rings of three words: level (or round) k reads slot k % 3, appends behind
+// itself counting in slot (k + 1) % 3, and zeroes slot (k + 2) % 3, which every CTA last read
+// before the barrier that opened level k, so one barrier per level suffices. Data other CTAs
+// write during the launch is read through L2 (ld.cg).
+constexpr int kIncThreads = 256;
+constexpr unsigned kIncSpins = 1u << 25;  // bounded barrier wait (a few seconds)
+enum { I_ERR = 0, I_CUTC = 1, I_QC = 4, I_NCUT = 8, I_ROUNDS = 9, I_RELAXED = 10, I_BAR = 32, I_WORDS = 64 };
+
+struct IncArgs {
+    const uint64_t* keys;
+    int64_t np;
+    CSRView fw, bw;
+    int32_t src;
+    int weighted;
+    uint64_t* st;
+    uint32_t* flag;
+    uint8_t* present;
+    int32_t* cut;
+    int32_t* q[2];
+    unsigned long long* ctl;  // I_* words, zeroed by the host; the barrier at I_BAR
+    int64_t max_rounds;
+};
+
+// Warp-uniform append: the warp's pushed values go to out[base + slot], slots from one atomicAdd.
+__device__ __forceinline__ void warp_push(bool push, int32_t v, int32_t* out, int64_t base, unsigned long long* cnt) {
+    const unsigned m = __ballot_sync(0xffffffffu, push);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned long long b0 = 0;
+    if (lane_id() == leader) b0 = atomicAdd(cnt, (unsigned long long)__popc(m));
+    b0 = __shfl_sync(0xffffffffu, b0, leader);
+    if (push) out[base + (int64_t)b0 + __popc(m & ((1u << lane_id()) - 1))] = v;
 }
+
+__global__ void __launch_bounds__(kIncThreads) k_inc_persistent(IncArgs a) {
+    unsigned long long* const ctl = a.ctl;
+    unsigned long long* const err = ctl + I_ERR;
+    unsigned int* const bar = reinterpret_cast<unsigned int*>(ctl + I_BAR);
+    const int ln = lane_id();
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+    const int64_t warp = tid >> 5, nwarps = nthr >> 5;
+    // 1. presence of every logged edge; 2a. an absent tree edge u -> v cuts v (cut level 0)
+    for (int64_t base = warp * 32; base < a.np; base += nwarps * 32) {
+        const int64_t i = base + ln;
+        bool push = false;
+        int32_t v = 0;
+        if (i < a.np) {
+            const int32_t u = (int32_t)(a.keys[i] >> 32);
+            v = (int32_t)(uint32_t)a.keys[i];
+            const int64_t b = a.fw.beg[u], e = b + a.fw.deg[u];
+            const int64_t k = lower_bound_dev(a.fw.adj, b, e, v);
+            const bool pr = k < e && a.fw.adj[k] == v;
+            a.present[i] = pr;
+            if (!pr && v != a.src) {
+                const uint64_t w = a.st[v];
+                push = w != kNone && parent_of(w) == u && atomicCAS(&a.flag[v], FLAG_CLEAR, FLAG_CUT) == FLAG_CLEAR;
+            }
+        }
+        warp_push(push, v, a.cut, 0, ctl + I_CUTC);
+    }
+    if (!grid_barrier(bar, err, kIncSpins)) return;
+    // 2b. the cut spreads down the dependence tree, level by level, behind itself in one list
+    int64_t lo = 0, hi = (int64_t)__ldcg(ctl + I_CUTC);
+    for (int k = 0; hi > lo; ++k) {
+        unsigned long long* const nc = ctl + I_CUTC + (k + 1) % 3;
+        if (tid == 0) ctl[I_CUTC + (k + 2) % 3] = 0ull;
+        for (int64_t i = lo + warp; i < hi; i += nwarps) {
+            const int32_t x = __ldcg(&a.cut[i]);
+            const int64_t b = a.fw.beg[x], e = b + a.fw.deg[x];
+            for (int64_t c = b; c < e; c += 32) {
+                bool push = false;
+                int32_t y = 0;
+                if (c + ln < e) {
+                    y = a.fw.adj[c + ln];
+                    if (y != a.src) {
+                        const uint64_t w = a.st[y];
+                        push = w != kNone && parent_of(w) == x &&
+                               atomicCAS(&a.flag[y], FLAG_CLEAR, FLAG_CUT) == FLAG_CLEAR;
+                    }
+                }
+                warp_push(push, y, a.cut, hi, nc);
+            }
+        }
+        if (!grid_barrier(bar, err, kIncSpins)) return;
+        lo = hi;
+        hi += (int64_t)__ldcg(nc);
+    }
+    const int64_t n_cut = hi;
+    // 3. the cut vertices restart from their best valid in-neighbour (cut words are skipped by flag)
+    for (int64_t i = tid; i < n_cut; i += nthr) a.st[__ldcg(&a.cut[i])] = kNone;
+    if (!grid_barrier(bar, err, kIncSpins)) return;
+    for (int64_t i = warp; i < n_cut; i += nwarps) {
+        const int32_t x = __ldcg(&a.cut[i]);
+        const int64_t b = a.bw.beg[x], e = b + a.bw.deg[x];
+        uint64_t best = kNone;
+        for (int64_t k = b + ln; k < e; k += 32) {
+            const int32_t p = a.bw.adj[k];
+            if (__ldcg(&a.flag[p]) == FLAG_CUT) continue;
+            const uint64_t kp = __ldcg(&a.st[p]);
+            if (kp == kNone) continue;
+            const uint64_t c = pack((kp >> 32) + weight_of(a.weighted, p, x), p);
+            best = c < best ? c : best;
+        }
+        best = warp_min_u64(best);
+        if (ln == 0) a.st[x] = best;
+    }
+    if (!grid_barrier(bar, err, kIncSpins)) return;
+    // 4a. the re-seeded cut vertices start the first frontier (round 0 counts in ring slot 0)
+    for (int64_t base = warp * 32; base < n_cut; base += nwarps * 32) {
+        const int64_t i = base + ln;
+        bool push = false;
+        int32_t x = 0;
+        if (i < n_cut) {
+            x = __ldcg(&a.cut[i]);
+            push = __ldcg(&a.st[x]) != kNone;
+            a.flag[x] = push ? FLAG_QUEUED : FLAG_CLEAR;
+        }
+        warp_push(push, x, a.q[0], 0, ctl + I_QC);
+    }
+    if (!grid_barrier(bar, err, kIncSpins)) return;
+    // 4b. logged edges present now relax once
+    for (int64_t base = warp * 32; base < a.np; base += nwarps * 32) {
+        const int64_t i = base + ln;
+        bool push = false;
+        int32_t v = 0;
+        if (i < a.np && __ldcg(&a.present[i])) {
+            const int32_t u = (int32_t)(a.keys[i] >> 32);
+            v = (int32_t)(uint32_t)a.keys[i];
+            const uint64_t k = __ldcg(&a.st[u]);
+            if (k != kNone) {
+                const uint64_t c = pack((k >> 32) + weight_of(a.weighted, u, v), u);
+                push = c < atomicMin((unsigned long long*)&a.st[v], (unsigned long long)c) &&
+                       atomicCAS(&a.flag[v], FLAG_CLEAR, FLAG_QUEUED) == FLAG_CLEAR;
+            }
+        }
+        warp_push(push, v, a.q[0], 0, ctl + I_QC);
+    }
+    if (!grid_barrier(bar, err, kIncSpins)) return;
+    // 5. propagation rounds: the frontier's flags are cleared before any of its distances is read
+    int64_t n = (int64_t)__ldcg(ctl + I_QC), r = 0, relaxed = 0;
+    for (; n > 0; ++r) {
+        if (r >= a.max_rounds) {
+            if (tid == 0) atomicExch(err, 2ull);  // (distances strictly fall: cannot happen)
+            return;
+        }
+        const int32_t* in = a.q[r & 1];
+        int32_t* out = a.q[(r + 1) & 1];
+        unsigned long long* const nc = ctl + I_QC + (r + 1) % 3;
+        if (tid == 0) ctl[I_QC + (r + 2) % 3] = 0ull;
+        relaxed += n;
+        for (int64_t i = tid; i < n; i += nthr) a.flag[__ldcg(&in[i])] = FLAG_CLEAR;
+        if (!grid_barrier(bar, err, kIncSpins)) return;
+        for (int64_t i = warp; i < n; i += nwarps) {
+            const int32_t x = __ldcg(&in[i]);
+            const int64_t b = a.fw.beg[x], e = b + a.fw.deg[x];
+            for (int64_t c = b; c < e; c += 32) {
+                bool push = false;
+                int32_t y = 0;
+                if (c + ln < e) {
+                    y = a.fw.adj[c + ln];
+                    const uint64_t cand = pack((__ldcg(&a.st[x]) >> 32) + weight_of(a.weighted, x, y), x);
+                    push = cand < __ldcg(&a.st[y]) &&
+                           cand < atomicMin((unsigned long long*)&a.st[y], (unsigned long long)cand) &&
+                           atomicCAS(&a.flag[y], FLAG_CLEAR, FLAG_QUEUED) == FLAG_CLEAR;
+                }
+                warp_push(push, y, out, 0, nc);
+            }
+        }
+        if (!grid_barrier(bar, err, kIncSpins)) return;
+        n = (int64_t)__ldcg(nc);
+    }
+    if (tid == 0) {
+        ctl[I_NCUT] = (unsigned long long)n_cut;
+        ctl[I_ROUNDS] = (unsigned long long)r;
+        ctl[I_RELAXED] = (unsigned long long)relaxed;
+    }
+}
+
 
 }  // namespace
 
@@ -317,70 +365,56 @@ int inc_update(gir_dev* g, int weighted) {
     };
     if ((rc = dev_alloc_n(g, &present, (size_t)np)) || (rc = dev_alloc_n(g, &flag, (size_t)V)) ||
         (rc = dev_alloc_n(g, &cut, (size_t)V)) || (rc = dev_alloc_n(g, &qa, (size_t)V)) ||
-        (rc = dev_alloc_n(g, &qb, (size_t)V)) || (rc = dev_alloc_n(g, &cnt, 4))) {
+        (rc = dev_alloc_n(g, &qb, (size_t)V)) || (rc = dev_alloc_n(g, &cnt, I_WORDS))) {
         cleanup();
         return rc;
     }
     int64_t launches = 0, rounds = 0, n_cut = 0, relaxed_from = 0;
-    auto launched = [&](const char* what) {
-        ++launches;
-        return cuda_check(g, cudaGetLastError(), what);
-    };
-    const CSRView fw = view(g->fw), bw = view(g->bw);
     do {
         if ((rc = cuda_check(g, cudaMemsetAsync(flag, 0, sizeof(uint32_t) * (size_t)V, g->stream), "inc flags")) ||
-            (rc = cuda_check(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 4, g->stream), "inc counters")))
+            (rc = cuda_check(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * I_WORDS, g->stream), "inc counters")))
             break;
-        k_inc_present<<<grid_for(g, np, kBlock), kBlock, 0, g->stream>>>(keys, np, fw, present);
-        if ((rc = launched("k_inc_present"))) break;
-        // 2. the cut, level by level into one list
-        k_inc_cut<<<grid_for(g, np, kBlock), kBlock, 0, g->stream>>>(keys, present, np, src, st, flag, cut, cnt);
-        if ((rc = launched("k_inc_cut"))) break;
-        int64_t lo = 0, hi = 0;
-        if ((rc = read_count(g, cnt, hc, &hi))) break;
-        while (hi > lo) {
-            k_inc_cut_level<<<grid_for(g, (hi - lo) * 32, kBlock), kBlock, 0, g->stream>>>(cut + lo, hi - lo, fw, src, st,
-                                                                                          flag, cut, cnt);
-            if ((rc = launched("k_inc_cut_level"))) break;
-            lo = hi;
-            if ((rc = read_count(g, cnt, hc, &hi))) break;
+        // one cooperative launch: every CTA of the grid must be resident at once
+        int per_sm = 0;
+        if ((rc = cuda_check(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_inc_persistent, kIncThreads, 0),
+                             "inc occupancy")))
+            break;
+        const int grid = g->num_sms * std::max(1, std::min(per_sm, 4));
+        IncArgs ia;
+        ia.keys = keys;
+        ia.np = np;
+        ia.fw = view(g->fw);
+        ia.bw = view(g->bw);
+        ia.src = src;
+        ia.weighted = weighted;
+        ia.st = st;
+        ia.flag = flag;
+        ia.present = present;
+        ia.cut = cut;
+        ia.q[0] = qa;
+        ia.q[1] = qb;
+        ia.ctl = cnt;
+        ia.max_rounds = V + 2;  // distances strictly fall, so every vertex is queued at most V times
+        void* kargs[] = {&ia};
+        if ((rc = cuda_check(g, cudaLaunchCooperativeKernel((const void*)k_inc_persistent, grid, kIncThreads, kargs, 0,
+                                                            g->stream), "k_inc_persistent")))
+            break;
+        ++launches;
+        if ((rc = cuda_check(g, cudaMemcpyAsync(hc, cnt, sizeof(unsigned long long) * 16, cudaMemcpyDeviceToHost, g->stream),
+                             "inc counters")) ||
+            (rc = cuda_check(g, cudaStreamSynchronize(g->stream), "inc update")))
+            break;
+        if (hc[I_ERR] == 2ull) {
+            rc = fail(g, GIR_ERR_TIMEOUT, "inc update: propagation did not converge");
+            break;
         }
-        if (rc) break;
-        n_cut = hi;
-        // 3. re-seed the cut from valid in-neighbours
-        if (n_cut > 0) {
-            k_inc_unset<<<grid_for(g, n_cut, kBlock), kBlock, 0, g->stream>>>(cut, n_cut, st);
-            if ((rc = launched("k_inc_unset"))) break;
-            k_inc_reseed<<<grid_for(g, n_cut * 32, kBlock), kBlock, 0, g->stream>>>(cut, n_cut, bw, flag, weighted, st);
-            if ((rc = launched("k_inc_reseed"))) break;
+        if (hc[I_ERR]) {
+            rc = fail(g, GIR_ERR_TIMEOUT, "inc update: a grid barrier ran out its bound");
+            break;
         }
-        // 4. seeds
-        if ((rc = cuda_check(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), g->stream), "inc counters"))) break;
-        if (n_cut > 0) {
-            k_inc_seed_cut<<<grid_for(g, n_cut, kBlock), kBlock, 0, g->stream>>>(cut, n_cut, st, flag, qa, cnt);
-            if ((rc = launched("k_inc_seed_cut"))) break;
-        }
-        k_inc_seed_edges<<<grid_for(g, np, kBlock), kBlock, 0, g->stream>>>(keys, present, np, weighted, st, flag, qa,
-                                                                            cnt);
-        if ((rc = launched("k_inc_seed_edges"))) break;
-        int64_t nq = 0;
-        if ((rc = read_count(g, cnt, hc, &nq))) break;
-        // 5. propagation rounds; distances strictly fall, so every vertex is queued at most V times
-        const int64_t max_rounds = V + 2;
-        while (nq > 0) {
-            if (++rounds > max_rounds) {
-                rc = fail(g, GIR_ERR_TIMEOUT, "inc update: propagation did not converge");
-                break;
-            }
-            relaxed_from += nq;
-            k_inc_unflag<<<grid_for(g, nq, kBlock), kBlock, 0, g->stream>>>(qa, nq, flag);
-            if ((rc = launched("k_inc_unflag"))) break;
-            if ((rc = cuda_check(g, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), g->stream), "inc counters"))) break;
-            k_inc_round<<<grid_for(g, nq * 32, kBlock), kBlock, 0, g->stream>>>(qa, nq, fw, weighted, st, flag, qb, cnt);
-            if ((rc = launched("k_inc_round"))) break;
-            std::swap(qa, qb);
-            if ((rc = read_count(g, cnt, hc, &nq))) break;
-        }
+        n_cut = (int64_t)hc[I_NCUT];
+        rounds = (int64_t)hc[I_ROUNDS];
+        relaxed_from = (int64_t)hc[I_RELAXED];
     } while (false);
     if (!rc) {
         g->inc_npend[m] = 0;

@@ -393,12 +393,22 @@ __global__ void k_bu_thread(const int32_t* ids, int64_t n, CSRView bw, const uin
             const uint64_t want = all & ~s;
             uint64_t nb = 0;
             if (want) {
+                // four row entries per step (rows start 16-byte aligned), their frontier masks
+                // loaded together; entries read past the point where every missing lane is found
+                // are in-neighbours all the same, so the lanes they add are found lanes too
                 uint64_t acc = 0;
                 const int64_t b = bw.beg[v], e = b + bw.deg[v];
-                for (int64_t k = b; k < e; ++k) {
-                    acc |= front[bw.adj[k]];
+                int64_t k = b;
+                for (; k + 4 <= e; k += 4) {
+                    const int4 a4 = *reinterpret_cast<const int4*>(bw.adj + k);
+                    acc |= front[a4.x] | front[a4.y] | front[a4.z] | front[a4.w];
                     if ((acc & want) == want) break;
                 }
+                if ((acc & want) != want)
+                    for (; k < e; ++k) {
+                        acc |= front[bw.adj[k]];
+                        if ((acc & want) == want) break;
+                    }
                 nb = acc & want;
             }
             next[v] = nb;

@@ -388,13 +388,14 @@ __global__ void __launch_bounds__(kRelaxThreads, kRelaxMinBlocks) k_relax(const 
                         const int32_t sel_lo = ln < pc ? nth_bit(mx, ln) : 0;
                         const int32_t sel_hi = ln + 32 < pc ? nth_bit(mx, ln + 32) : 0;
                         const int da = kStep / pc, db = kStep % pc;
-                        int64_t e[kPairs];
+                        int64_t e[kPairs];  // the pair's entry of the weight-sorted rows (ebx + edge)
                         int r[kPairs];
     #pragma unroll
                         for (int j = 0; j < kPairs; ++j) {
                             const int64_t q2 = p + j * 32 + ln - px;
-                            e[j] = q2 / pc;
-                            r[j] = (int)(q2 - e[j] * pc);
+                            const int64_t ed = q2 / pc;
+                            r[j] = (int)(q2 - ed * pc);
+                            e[j] = ebx + ed;
                         }
                         for (; p + kStep <= xend; p += kStep) {
                             bool on[kPairs];
@@ -407,8 +408,8 @@ __global__ void __launch_bounds__(kRelaxThreads, kRelaxMinBlocks) k_relax(const 
                                 const int32_t hi = __shfl_sync(0xffffffffu, sel_hi, r[j] & 31);
                                 sl[j] = r[j] < 32 ? lo : hi;
                                 on[j] = true;
-                                w[j] = __ldcs(&a.wadj[ebx + e[j]]);
-                                wt[j] = __ldcs(&a.ww[ebx + e[j]]);
+                                w[j] = __ldcs(&a.wadj[e[j]]);
+                                wt[j] = __ldcs(&a.ww[e[j]]);
                                 du[j] = dist[urow + sl[j]];
                                 e[j] += da;
                                 r[j] += db;

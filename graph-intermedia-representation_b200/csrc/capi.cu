@@ -489,7 +489,9 @@ static int single_fast(gir_dev* g, const int32_t* u, const int32_t* v, const uin
     fl[F_DAG] = (bits >> 2) & 1;
     fl[F_BCT] = (bits >> 3) & 1;
     const uint64_t one_key = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
-    return plan_and_repair(g, fl, symc == 1 ? 2 : 0, symc == 2 ? 2 : 0, keys + 1, insert, !insert, one_key);
+    // (a pair that appeared inside one weakly connected component unions nothing)
+    const int64_t nsi = symc == 1 && !((bits >> 4) & 1) ? 2 : 0;
+    return plan_and_repair(g, fl, nsi, symc == 2 ? 2 : 0, keys + 1, insert, !insert, one_key);
 }
 
 // sync (gir.cpp:3602-3632): the layers catch up with every batch ingested since the last sync,

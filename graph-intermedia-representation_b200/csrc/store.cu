@@ -309,12 +309,14 @@ struct MutCSR {
 // runs instead). out[1]: 1 when the undirected pair {u, v} appeared, 2 when it disappeared.
 // out[2]: layer flags judged with the current labels, as the batch classification does (bit 0
 // an edge inside an SCC deleted, bit 1 an inserted cross edge against the rank order, bit 2 a
-// cross edge changed, bit 3 the blocks may change). keys: u << 32 | v, then the two orientations
-// of the pair.
+// cross edge changed, bit 3 the blocks may change, bit 4 an undirected pair appeared between two
+// vertices that already share a weakly connected component, so the WCC labels stand). keys:
+// u << 32 | v, then the two orientations of the pair.
 __global__ void __launch_bounds__(1024) k_single_edit(MutCSR fw, MutCSR bw, MutCSR sym, int32_t u, int32_t v, int insert,
                                                       int weights, uint64_t wseed, uint32_t wlo, uint32_t whi,
                                                       const int32_t* scc, const int32_t* rank, const int32_t* blk,
-                                                      const int32_t* head, unsigned long long* out, uint64_t* keys) {
+                                                      const int32_t* head, const int32_t* wcc, unsigned long long* out,
+                                                      uint64_t* keys) {
     __shared__ int64_t s_pos[4];
     __shared__ int s_st, s_sym;
     if (threadIdx.x == 0) {
@@ -354,6 +356,7 @@ __global__ void __launch_bounds__(1024) k_single_edit(MutCSR fw, MutCSR bw, MutC
                 }
             }
         }
+        if (st == 1 && symc == 1 && wcc && wcc[u] == wcc[v]) fl |= 16;
         s_pos[0] = pf; s_pos[1] = pb; s_pos[2] = psu; s_pos[3] = psv;
         s_st = st;
         s_sym = symc;
@@ -405,9 +408,10 @@ int store_single_edit(gir_dev* g, int32_t u, int32_t v, int insert, unsigned lon
     const int32_t* rank = g->scc_built ? static_cast<const int32_t*>(g->scc_rank.p) : nullptr;
     const int32_t* blk = g->bct_built ? static_cast<const int32_t*>(g->blk_label.p) : nullptr;
     const int32_t* head = g->bct_built ? static_cast<const int32_t*>(g->blk_head.p) : nullptr;
+    const int32_t* wcc = g->wcc_built ? static_cast<const int32_t*>(g->wcc.p) : nullptr;
     k_single_edit<<<1, 1024, 0, g->stream>>>(mut(g->fw), mut(g->bw), mut(g->sym), u, v, insert,
                                              g->has_weights && g->fw.w ? 1 : 0, g->wrule_seed, g->wrule_lo, g->wrule_hi,
-                                             scc, rank, blk, head, out, keys);
+                                             scc, rank, blk, head, wcc, out, keys);
     GIR_LAUNCH(g, "k_single_edit");
     return GIR_OK;
 }

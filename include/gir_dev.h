@@ -204,7 +204,9 @@ int gir_dev_bc(gir_dev_t* g, const int32_t* srcs, int64_t n_src, double* score_o
  * = the level / distance of v, UINT64_MAX = unreachable; GIR_ERR_STATE when the mode was never
  * tracked. A source out of range tracks an all-unreachable result, as GIR::bfs / sssp give one.
  * After an update, gir_dev_query_stats gives: iterations = propagation rounds, reached = vertices
- * whose tree edge was cut (and their subtrees), edges = frontier entries relaxed. */
+ * whose tree edge was cut (and their subtrees), edges = frontier entries relaxed. An update is one
+ * cooperative launch over every co-resident CTA (its phases meet at grid barriers whose waits are
+ * bounded: GIR_ERR_TIMEOUT if one runs out), read back once at the end. */
 int gir_dev_inc_track(gir_dev_t* g, int32_t source, int weighted);
 int gir_dev_inc_update(gir_dev_t* g, int weighted);
 int gir_dev_inc_dist(gir_dev_t* g, int weighted, uint64_t* dist_out);

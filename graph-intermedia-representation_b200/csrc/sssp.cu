@@ -561,26 +561,58 @@ __global__ void k_sssp_reached(const D* dist, int64_t V, int nl, const int32_t* 
     }
 }
 
-// dist[v * nl + s] -> out[row[s] * V + v], through 32 x 32 shared-memory tiles.
+// dist[v * nl + s] -> out[row[s] * V + v], through 32 x 32 shared-memory tiles, a fixed grid
+// striding over the tiles. On the way it counts what k_sssp_reached counts (reached (vertex, lane)
+// pairs and their out-edges) from the same coalesced loads, with one atomicAdd per CTA.
 template <class D>
-__global__ void k_transpose(const D* dist, int64_t V, int nl, const int64_t* row, uint64_t* out) {
+__global__ void k_transpose(const D* dist, int64_t V, int nl, const int64_t* row, const int32_t* outdeg,
+                            uint64_t* out, unsigned long long* cnt) {
     __shared__ uint64_t tile[32][33];
-    const int64_t v0 = (int64_t)blockIdx.x * 32;
-    const int s0 = blockIdx.y * 32;
+    __shared__ unsigned long long s_r[8], s_e[8];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
-    for (int r = ty; r < 32; r += 8) {
-        const int64_t v = v0 + r;
-        const int s = s0 + tx;
-        if (v < V && s < nl) {
-            const D d = dist[v * nl + s];
-            tile[r][tx] = d == DistT<D>::inf ? kInf : (uint64_t)d;
+    const int64_t tiles_v = (V + 31) / 32, tiles_s = (nl + 31) / 32;
+    unsigned long long r_cnt = 0, e_cnt = 0;
+    for (int64_t t = blockIdx.x; t < tiles_v * tiles_s; t += gridDim.x) {
+        const int64_t v0 = (t % tiles_v) * 32;
+        const int s0 = (int)(t / tiles_v) * 32;
+        for (int r = ty; r < 32; r += 8) {
+            const int64_t v = v0 + r;
+            const int s = s0 + tx;
+            if (v < V && s < nl) {
+                const D d = dist[v * nl + s];
+                const bool fin = d != DistT<D>::inf;
+                tile[r][tx] = fin ? (uint64_t)d : kInf;
+                if (fin) {
+                    ++r_cnt;
+                    e_cnt += (unsigned long long)outdeg[v];
+                }
+            }
         }
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const int s = s0 + r;
+            const int64_t v = v0 + tx;
+            if (v < V && s < nl) out[row[s] * V + v] = tile[tx][r];
+        }
+        __syncthreads();
+    }
+    for (int o = 16; o; o >>= 1) {
+        r_cnt += __shfl_xor_sync(0xffffffffu, r_cnt, o);
+        e_cnt += __shfl_xor_sync(0xffffffffu, e_cnt, o);
+    }
+    if (tx == 0) {
+        s_r[ty] = r_cnt;
+        s_e[ty] = e_cnt;
     }
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        const int s = s0 + r;
-        const int64_t v = v0 + tx;
-        if (v < V && s < nl) out[row[s] * V + v] = tile[tx][r];
+    if (threadIdx.x == 0) {
+        unsigned long long rr = 0, ee = 0;
+        for (int k = 0; k < 8; ++k) {
+            rr += s_r[k];
+            ee += s_e[k];
+        }
+        if (rr) atomicAdd(&cnt[S_REACHED], rr);
+        if (ee) atomicAdd(&cnt[S_EDGES], ee);
     }
 }
 
@@ -840,12 +872,12 @@ int sssp_group(gir_dev* g, Work& wk, const DevCSR& ws, int nl, const int64_t* la
             return GIR_OK;
         }
     }
-    k_sssp_reached<D><<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(dist, V, nl, g->fw.deg, cnt);
-    GIR_LAUNCH(g, "k_sssp_reached");
-    if (!direct) {
-        dim3 grd((unsigned)((V + 31) / 32), (unsigned)((nl + 31) / 32));
-        k_transpose<D><<<grd, 256, 0, g->stream>>>(dist, V, nl, lane_row_d, out);
+    if (!direct) {  // (the transpose also counts the reached pairs and their edges)
+        k_transpose<D><<<g->num_sms * 8, 256, 0, g->stream>>>(dist, V, nl, lane_row_d, g->fw.deg, out, cnt);
         GIR_LAUNCH(g, "k_transpose");
+    } else {
+        k_sssp_reached<D><<<grid_for(g, V, kBlock), kBlock, 0, g->stream>>>(dist, V, nl, g->fw.deg, cnt);
+        GIR_LAUNCH(g, "k_sssp_reached");
     }
     return GIR_OK;
 }

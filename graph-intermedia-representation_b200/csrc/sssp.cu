@@ -209,7 +209,8 @@ __global__ void k_light_split(int64_t V, const int64_t* wb, const int32_t* wdeg,
 
 // Takes every queued vertex's lanes (clearing them), does the settle bookkeeping and writes queue
 // entry i's item (vertex, first edge, lane mask, work = edges x lanes) into slot i; cnt[S_ITEMS]
-// = n and pref[n] = 0, so the scan of the n + 1 slots needs nothing cleared beforehand. Items
+// = n and pref[n] = 0, so the scan of the n + 1 slots needs nothing cleared beforehand (and the
+// near-queue counter starts the pass at zero). Items
 // without work stay in place: the relaxation's searches take the largest item whose prefix is at
 // most the pair's index, which is never a zero-work item (its prefix equals the next item's).
 // A vertex is queued once per pass, so its setmask word is touched by one thread only.
@@ -254,6 +255,7 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         it.pref[n] = 0;
         a.cnt[S_ITEMS] = (unsigned long long)n;
+        a.cnt[S_NEAR] = 0ull;  // the pass's near appends count from zero (the host read the last count)
     }
 }
 
@@ -817,7 +819,6 @@ int sssp_group(gir_dev* g, Work& wk, const DevCSR& ws, int nl, const int64_t* la
         GIR_CUDA(g, cudaMemsetAsync(cnt + S_SET, 0, sizeof(unsigned long long), g->stream));
         // light rounds: nearq (lanes in curmask) -> nextq (lanes in nextmask)
         while (n_near > 0) {
-            GIR_CUDA(g, cudaMemsetAsync(cnt + S_NEAR, 0, sizeof(unsigned long long), g->stream));
             a.curmask = curmask; a.nextmask = nextmask; a.nextq = nextq; a.farq = farq;
             GIR_TRY(relax(nearq, n_near, 0));
             st.iterations++;

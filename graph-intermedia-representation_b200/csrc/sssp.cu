@@ -262,7 +262,8 @@ __global__ void k_relax_prep(const int32_t* q, int64_t n, int heavy, Relax a, co
 constexpr int kRelaxThreads = 256;
 // Pairs per thread per step, and CTAs per SM: latency-bound, so occupancy wins. Measured on the
 // 4.8M-vertex R-MAT (64 lanes): 1 pair at 8 CTAs (32 registers) 71 ms per call, 7 CTAs the same,
-// 6 CTAs 75 ms, 4 CTAs 83 ms; 2 pairs at 6 CTAs 74 ms, at 5 CTAs 76 ms.
+// 6 CTAs 75 ms, 4 CTAs 83 ms; 2 pairs at 6 CTAs 74 ms, at 5 CTAs 76 ms. (With the later changes:
+// 256-thread CTAs 66.3 ms, 128-thread CTAs at 16 per SM 66.8 ms.)
 constexpr int kPairs = 1;
 constexpr int kRelaxMinBlocks = 8;
 constexpr int kDeal = 8;  // chunks of pairs per warp and launch, at least 32 pairs each (measured on
